@@ -1,0 +1,333 @@
+# -*- coding: utf-8 -*-
+"""CPU float64 restatement of ssqueezepy's synchrosqueezing hot path.
+
+TEST INFRASTRUCTURE ONLY. This module is the checker: only `tests/`,
+`__graft_entry__.smoke()` and the CPU-baseline / reference arm of `bench.py`
+may import it. The product (`ssqueezepy_b200`) never calls it and has no CPU
+fallback.
+
+Each function restates the reference routine it cites (paths relative to the
+ssqueezepy source tree) in plain numpy / scipy.fft, float64 throughout, the
+way ssqueezepy computes with a float64 `Wavelet`. It is pinned against
+outputs of ssqueezepy itself: tests/golden/*.npz, generated by
+tests/golden/make_golden.py (see tests/test_oracle.py).
+
+Host parameters (scales, ssq_freqs, per-row weights) are inputs here; they
+are pinned separately against the same fixtures (tests/test_params.py).
+"""
+import os
+import numpy as np
+from concurrent.futures import ThreadPoolExecutor
+from scipy import fft as sfft
+
+PI = np.pi
+EPS32 = float(np.finfo(np.float32).eps)
+EPS64 = float(np.finfo(np.float64).eps)
+_WORKERS = os.cpu_count() or 1
+
+
+#### padding (utils/common.py:32-51, 54-158) ##################################
+def p2up(n):
+    up = int(2 ** (1 + np.round(np.log2(n))))
+    n2 = (up - n) // 2
+    return up, up - n - n2, n2
+
+
+def pad(x, padtype, n1, n2):
+    """Pad the last axis by (n1, n2) with numpy's modes, as padsignal does."""
+    widths = [(0, 0)] * (x.ndim - 1) + [(n1, n2)]
+    if padtype == 'zero':
+        return np.pad(x, widths)
+    if padtype == 'reflect':
+        return np.pad(x, widths, mode='reflect')
+    if padtype == 'replicate':
+        return np.pad(x, widths, mode='edge')
+    if padtype == 'wrap':
+        return np.pad(x, widths, mode='wrap')
+    if padtype == 'symmetric':
+        r = x[..., ::-1]
+        return np.concatenate([r[..., r.shape[-1] - n1:], x, r[..., :n2]], -1)
+    raise ValueError(padtype)
+
+
+#### wavelets (wavelets.py:473-530, _gmw.py:187-251) ##########################
+def xi_grid(N):
+    """[0, .., N//2, -(N-N//2-1), .., -1] * 2pi/N (wavelets.py:473-484)."""
+    h = 2 * PI / N
+    k = np.arange(N, dtype=np.float64)
+    k[N // 2 + 1:] -= N
+    return k * h
+
+
+def psih(kind, params, w):
+    """Frequency-domain wavelet at radian frequencies `w`.
+
+    kind 'morlet': params (mu,): C1*(exp(-(w-mu)^2/2) - ks*exp(-w^2/2)),
+      ks = exp(-mu^2/2), C1 = sqrt(2)*cs*pi^(1/4),
+      cs = (1 + exp(-mu^2) - 2exp(-3mu^2/4))^(-1/2)   (wavelets.py:498-527)
+    kind 'gmw_l1': params (gamma, beta): 2exp(-beta ln wc + wc^gamma
+      + beta ln w - w^gamma) for w >= 0, wc = (beta/gamma)^(1/gamma)
+                                                     (_gmw.py:187-210, 638)
+    kind 'gmw_l2': params (gamma, beta): sqrt(2pi gamma 2^r / Gamma(r))
+      w^beta exp(-w^gamma), r = (2beta+1)/gamma      (_gmw.py:228-251)
+    """
+    w = np.asarray(w, dtype=np.float64)
+    if kind == 'morlet':
+        mu, = params
+        cs = (1 + np.exp(-mu**2) - 2 * np.exp(-3 / 4 * mu**2)) ** (-.5)
+        ks = np.exp(-.5 * mu**2)
+        C1 = np.sqrt(2) * cs * PI**.25
+        return C1 * (np.exp(-.5 * (w - mu)**2) - ks * np.exp(-.5 * w**2))
+    gamma, beta = params
+    wc = (beta / gamma) ** (1 / gamma)
+    nonneg = w >= 0
+    w = w * nonneg
+    with np.errstate(divide='ignore'):
+        if kind == 'gmw_l1':
+            return 2 * np.exp(-beta * np.log(wc) + wc**gamma
+                              + beta * np.log(w) - w**gamma) * nonneg
+        from scipy.special import gamma as gamma_fn
+        r = (2 * beta + 1) / gamma
+        return (np.sqrt(2. * PI * gamma * 2.**r / gamma_fn(r))
+                * w**beta * np.exp(-w**gamma) * nonneg)
+    raise ValueError(kind)
+
+
+def psih_bank(kind, params, scales, Npad):
+    """psih(scale * xi) for every scale, Nyquist bin halved for even Npad
+    (wavelets.py:62-95, _cwt.py:167-171 with nohalf=False)."""
+    xi = xi_grid(Npad)
+    P = psih(kind, params, np.asarray(scales, np.float64).reshape(-1, 1) * xi)
+    if Npad % 2 == 0:
+        P[:, Npad // 2] /= 2
+    return P, xi
+
+
+#### CWT (_cwt.py:167-177, 246-320) ###########################################
+def cwt(x, kind, params, scales, dt=1., padtype='reflect', l1_norm=True,
+        derivative=True):
+    """Wx (and dWx) of 1D or 2D `x`, shape (..., na, N)."""
+    x = np.asarray(x, dtype=np.float64)
+    N = x.shape[-1]
+    if padtype is None:
+        Npad, n1 = N, 0
+        xp = x
+    else:
+        Npad, n1, n2 = p2up(N)
+        xp = pad(x, padtype, n1, n2)
+    xh = sfft.fft(xp, axis=-1, workers=_WORKERS)
+    P, xi = psih_bank(kind, params, scales, Npad)
+    if x.ndim == 2:
+        xh = xh[:, None]
+    Pxh = P * xh
+    Wx = sfft.ifft(Pxh, axis=-1, workers=_WORKERS)[..., n1:n1 + N]
+    dWx = None
+    if derivative:
+        Pxh *= (1j * xi / dt)
+        dWx = sfft.ifft(Pxh, axis=-1, workers=_WORKERS)[..., n1:n1 + N]
+    if not l1_norm:
+        s = np.sqrt(np.asarray(scales, np.float64).reshape(-1, 1))
+        Wx = Wx * s
+        if dWx is not None:
+            dWx = dWx * s
+    return np.ascontiguousarray(Wx), (None if dWx is None else
+                                      np.ascontiguousarray(dWx))
+
+
+#### phase transform (algos.py:706-740, 784-816) ##############################
+def phase_cwt(Wx, dWx, gamma):
+    """|Im(dWx conj(Wx))| / (|Wx|^2 2pi); inf where |Wx| < gamma."""
+    A, B = dWx.real, dWx.imag
+    C, D = Wx.real, Wx.imag
+    with np.errstate(divide='ignore', invalid='ignore'):
+        w = np.abs((B * C - A * D) / ((C**2 + D**2) * 6.283185307179586))
+    w[np.abs(Wx) < gamma] = np.inf
+    return w
+
+
+def phase_stft(Sx, dSx, Sfs, gamma):
+    """|Sfs_i - Im(dS conj(S)) / (|S|^2 2pi)|; inf where |S| < gamma."""
+    A, B = dSx.real, dSx.imag
+    C, D = Sx.real, Sx.imag
+    Sfs = np.asarray(Sfs, np.float64).reshape(-1, 1)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        w = np.abs(Sfs - (B * C - A * D) / ((C**2 + D**2) * 6.283185307179586))
+    w[np.abs(Sx) < gamma] = np.inf
+    return w
+
+
+#### bins (algos.py:356-374, 859-984) #########################################
+def transition_idx(v):
+    """Split index of two log-spaced pieces, or None (cwt_utils.py:375-394)."""
+    v = np.asarray(v)
+    d2 = np.abs(np.diff(np.log(v), 2, axis=0)).ravel()
+    idx = int(np.argmax(d2)) + 2
+    mx = d2.max()
+    d2[idx - 2] = 0
+    th = 1e-14 if v.dtype == np.float64 else 1e-6
+    if not np.any(mx > 100 * np.abs(d2).mean()):
+        return None
+    if not np.all(np.abs(d2) < th):
+        return None
+    return idx
+
+
+def bin_index(w, ssq_freqs, logscale, flipud):
+    """Frequency bin of each phase-transform value (round-half-even as numba's
+    `round`); `w` must be finite where used."""
+    v = np.asarray(ssq_freqs, np.float64).ravel()
+    omax = len(v) - 1
+    with np.errstate(divide='ignore', invalid='ignore'):
+        if not logscale:
+            dv = max(float(v[1] - v[0]), EPS64)
+            k = np.minimum(np.round(np.maximum((w - v[0]) / dv, 0)), omax)
+        else:
+            idx = transition_idx(v)
+            vlmin = float(np.log2(v[0]))
+            wl = np.log2(w)
+            if idx is None:
+                dvl = max(float(np.log2(v[1]) - np.log2(v[0])), EPS64)
+                k = np.minimum(np.round(np.maximum((wl - vlmin) / dvl, 0)), omax)
+            else:
+                vlmin1 = float(np.log2(v[idx - 1]))
+                dvl0 = max(float(np.log2(v[1]) - np.log2(v[0])), EPS64)
+                dvl1 = max(float(np.log2(v[idx]) - np.log2(v[idx - 1])), EPS64)
+                hi = np.minimum(np.round((wl - vlmin1) / dvl1) + (idx - 1), omax)
+                lo = np.maximum(np.round((wl - vlmin) / dvl0), 0)
+                k = np.where(wl > vlmin1, hi, lo)
+    k = np.where(np.isfinite(k), k, 0).astype(np.int64)
+    if flipud:
+        k = omax - k
+    return k
+
+
+def squeeze(Wx, k, use, const):
+    """Tx[k[i,j], j] += Wx[i,j]*const[i] over i ascending, for `use` entries.
+
+    `np.bincount` accumulates in input order, so each bin receives rows in
+    ascending i, the reference's per-column order (algos.py:879-895)."""
+    na, N = Wx.shape
+    const = np.broadcast_to(np.asarray(const, np.float64).ravel(), (na,))
+    V = Wx * const[:, None]
+    out = np.empty((na, N), dtype=np.complex128)
+
+    def block(j0, j1):
+        kk = k[:, j0:j1]
+        uu = use[:, j0:j1]
+        cols = np.broadcast_to(np.arange(j1 - j0), kk.shape)
+        lin = (kk * (j1 - j0) + cols)[uu]
+        vv = V[:, j0:j1][uu]
+        re = np.bincount(lin, weights=vv.real, minlength=na * (j1 - j0))
+        im = np.bincount(lin, weights=vv.imag, minlength=na * (j1 - j0))
+        out[:, j0:j1] = (re + 1j * im).reshape(na, j1 - j0)
+
+    step = max(256, -(-N // (4 * _WORKERS)))
+    spans = [(j, min(N, j + step)) for j in range(0, N, step)]
+    if len(spans) == 1:
+        block(*spans[0])
+    else:
+        with ThreadPoolExecutor(_WORKERS) as ex:
+            list(ex.map(lambda s: block(*s), spans))
+    return out
+
+
+def ssq_cwt(x, kind, params, scales, ssq_freqs, const, dt=1.,
+            padtype='reflect', logscale=True, flipud=True, gamma=None):
+    """(Tx, Wx, w) of `ssq_cwt` for 1D or 2D `x`; `ssq_freqs` ascending, as
+    passed to the squeeze (ssqueezing.py:122-146, 204-214)."""
+    Wx, dWx = cwt(x, kind, params, scales, dt=dt, padtype=padtype)
+    gamma = 10 * EPS64 if gamma is None else gamma
+    if Wx.ndim == 2:
+        w = phase_cwt(Wx, dWx, gamma)
+        use = np.abs(Wx) > gamma
+        k = bin_index(np.where(use, w, 1.), ssq_freqs, logscale, flipud)
+        return squeeze(Wx, k, use, const), Wx, w
+    outs = [ssq_cwt(xi_, kind, params, scales, ssq_freqs, const, dt, padtype,
+                    logscale, flipud, gamma) for xi_ in x]
+    return tuple(np.stack(o) for o in zip(*outs))
+
+
+#### STFT (_stft.py:127-181, utils/stft_utils.py:20-98) #######################
+def frames(xp, n_fft, hop, modulated=True):
+    """(n_fft, n_frames) frame matrix; modulated frames are rotated by
+    ceil(n_fft/2) (stft_utils.py:69-82)."""
+    n_segs = (xp.shape[-1] - n_fft) // hop + 1
+    s20 = int(np.ceil(n_fft / 2))
+    s21 = s20 - 1 if n_fft % 2 == 1 else s20
+    starts = hop * np.arange(n_segs)
+    m = np.arange(n_fft)
+    if modulated:
+        src = np.where(m < s20, m + s21, m - s20)
+    else:
+        src = m
+    return xp[..., starts[None, :] + src[:, None]]
+
+
+def stft(x, window, diff_window, n_fft, hop=1, fs=1., padtype='reflect',
+         modulated=True):
+    """(Sx, dSx), each (n_fft//2+1, n_frames) (or batched)."""
+    x = np.asarray(x, np.float64)
+    N = x.shape[-1]
+    padlength = N + n_fft - 1
+    if abs(padlength - N) % 2 == 0:
+        n1 = n2 = (padlength - N) // 2
+    else:
+        n2 = (padlength - N) // 2
+        n1 = n2 + 1
+    xp = pad(x, padtype, n1, n2)
+    F = frames(xp, n_fft, hop, modulated)
+    win = np.asarray(window, np.float64)
+    dwin = np.asarray(diff_window, np.float64) * fs
+    if modulated:
+        win, dwin = np.fft.ifftshift(win), np.fft.ifftshift(dwin)
+    ax = -2
+    shp = (-1, 1)
+    Sx = sfft.rfft(F * win.reshape(shp), axis=ax, workers=_WORKERS)
+    dSx = sfft.rfft(F * dwin.reshape(shp), axis=ax, workers=_WORKERS)
+    return Sx, dSx
+
+
+def ssq_stft(x, window, diff_window, n_fft, hop=1, fs=1., padtype='reflect',
+             modulated=True, flipud=False, gamma=None):
+    """(Tx, Sx, w, Sfs) of `ssq_stft` (_ssq_stft.py:88-136)."""
+    Sx, dSx = stft(x, window, diff_window, n_fft, hop, fs, padtype, modulated)
+    gamma = 10 * EPS64 if gamma is None else gamma
+    nrow = Sx.shape[-2]
+    Sfs = np.linspace(0, .5 * fs, nrow)
+    const = Sfs[1] - Sfs[0]
+    if Sx.ndim == 2:
+        w = phase_stft(Sx, dSx, Sfs, gamma)
+        use = np.abs(Sx) > gamma
+        k = bin_index(np.where(use, w, 0.), Sfs, False, flipud)
+        return squeeze(Sx, k, use, const), Sx, w, Sfs
+    outs = [ssq_stft(xi_, window, diff_window, n_fft, hop, fs, padtype,
+                     modulated, flipud, gamma) for xi_ in x]
+    Tx, S, w, _ = zip(*outs)
+    return np.stack(Tx), np.stack(S), np.stack(w), Sfs
+
+
+#### inverse CWT, one integral (_cwt.py:406-453, 479-494) #####################
+def icwt(Wx, scales, scaletype, nv, Cpsi, x_mean=0., l1_norm=True):
+    """x = (2/Cpsi) * sum over log pieces of (ln2/nv_p) sum_i Re Wx_i
+    [/scale_i for linear] + x_mean; `nv` per row (log-piecewise) or scalar.
+
+    For log-piecewise scales the reference recurses once per piece and each
+    piece adds `x_mean` (_cwt.py:422-429, 452), so the mean enters twice."""
+    scales = np.asarray(scales, np.float64).ravel()
+    if scaletype == 'log-piecewise':
+        idx = transition_idx(scales)
+        nvs = np.asarray(nv, np.float64).ravel()
+        return (icwt(Wx[..., :idx, :], scales[:idx], 'log', nvs[0], Cpsi,
+                     x_mean, l1_norm) +
+                icwt(Wx[..., idx:, :], scales[idx:], 'log', nvs[idx], Cpsi,
+                     x_mean, l1_norm))
+    if scaletype == 'log':
+        norm = np.ones_like(scales) if l1_norm else scales**.5
+    else:
+        norm = scales if l1_norm else scales**1.5
+    x = (Wx.real / norm.reshape(-1, 1)).sum(axis=-2)
+    if scaletype == 'log':
+        x = x * ((2 / Cpsi) * np.log(2 ** (1 / float(np.round(nv)))))
+    else:
+        x = x * ((2 / Cpsi) * PI / 4)
+    return x + x_mean

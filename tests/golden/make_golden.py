@@ -1,0 +1,188 @@
+# -*- coding: utf-8 -*-
+"""Generate the golden fixtures under tests/golden/ by running ssqueezepy
+itself (float64 path, CPU, numba) on seeded inputs.
+
+Usage (needs the ssqueezepy source tree; only run where it exists):
+
+    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py \
+        /path/to/ssqueezepy-checkout
+
+Writes:
+  host_params.npz  scales / ssq_freqs / bin parameters / adm_ssq for many
+                   (wavelet, N, scheme) combinations
+  transforms.npz   small end-to-end ssq_cwt / cwt / ssq_stft / stft / icwt
+                   outputs (float64) with their inputs
+  digests.npz      full-size (N=10,000 and N=160,000) float64 digests: row
+                   norms and row sums of Wx and Tx, total norms, and a bin
+                   histogram, for size-independent checks
+"""
+import os
+import sys
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def chirp_signal(N, seed=0):
+    """Linear chirp 0.01->0.2 cycles/sample + AM tone at 0.3 + N(0, 0.1^2)
+    noise; the 10k / 160k single-signal workload."""
+    t = np.arange(N, dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    x = (np.cos(2 * np.pi * (0.01 * t + 0.19 * t**2 / (2 * N)))
+         + (0.5 + 0.5 * np.cos(2 * np.pi * 0.001 * t)) * np.cos(2 * np.pi * 0.3 * t)
+         + 0.1 * rng.standard_normal(N))
+    return x
+
+
+def main(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    os.environ.setdefault('SSQ_PARALLEL', '1')
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    from ssqueezepy import Wavelet
+    from ssqueezepy.utils import (process_scales, p2up, adm_ssq,
+                                  logscale_transition_idx)
+    from ssqueezepy.ssqueezing import _compute_associated_frequencies
+    from ssqueezepy.algos import _get_params_find_closest_log
+
+    wavs = {
+        'morlet6': ('morlet', {'mu': 6.}),
+        'morlet13.4': ('morlet', {'mu': 13.4}),
+        'morlet5': ('morlet', {'mu': 5.}),
+        'gmw3_60': ('gmw', {'gamma': 3., 'beta': 60.}),
+        'gmw3_8': ('gmw', {'gamma': 3., 'beta': 8.}),
+    }
+
+    def W(key):
+        name, opts = wavs[key]
+        return Wavelet((name, dict(opts, dtype='float64')))
+
+    #### host params ##########################################################
+    hp = {}
+    Ns = [64, 100, 256, 300, 1000, 2048, 4096, 10000, 16384, 65536, 160000,
+          1048576]
+    for key in wavs:
+        w = W(key)
+        hp[f'adm_ssq/{key}'] = np.array(adm_ssq(w))
+        for N in Ns:
+            hp[f'p2up/{N}'] = np.array(p2up(N))
+            for st in ('log', 'log-piecewise', 'linear', 'log:maximal',
+                       'log:minimal'):
+                try:
+                    s = process_scales(st, N, w, nv=32)
+                except Exception:
+                    hp[f'scales/{key}/{N}/{st}'] = np.array([])  # raises
+                    continue
+                s1 = s.ravel()
+                if s1.size > 2048:  # long linear grids: keep ends + digest
+                    hp[f'scales_digest/{key}/{N}/{st}'] = np.array(
+                        [s1.size, s1.sum(), (s1 * s1).sum()])
+                    s1 = np.hstack([s1[:64], s1[-64:]])
+                hp[f'scales/{key}/{N}/{st}'] = s1
+                if N not in (256, 10000, 160000):
+                    continue
+                for sqs in ('log', 'log-piecewise', 'linear'):
+                    for mr in ('peak', 'energy', 'maximal'):
+                        if mr == 'maximal' and sqs == 'log-piecewise':
+                            continue
+                        try:
+                            f = _compute_associated_frequencies(
+                                s, N, w, sqs, mr, True, 1., 'cwt')
+                        except Exception:
+                            continue
+                        k = f'ssq_freqs/{key}/{N}/{st}/{sqs}/{mr}'
+                        hp[k] = (f if f.size <= 2048 else
+                                 np.hstack([f[:64], f[-64:]]))
+                        if sqs.startswith('log'):
+                            _, p = _get_params_find_closest_log(f)
+                            hp['binp/' + k[10:]] = np.array(
+                                [float(v) for v in p.values()])
+        hp[f'nv32/{key}'] = np.array(32)
+    np.savez_compressed(os.path.join(HERE, 'host_params.npz'), **hp)
+    print('host_params', len(hp))
+
+    #### small end-to-end transforms ########################################
+    tr = {}
+    cases = [
+        # name, N, wavelet, scales, ssq_freqs, maprange, padtype, flipud
+        ('c0', 256, 'morlet6', 'log-piecewise', 'log', 'peak', 'reflect', True),
+        ('c1', 160, 'gmw3_60', 'log-piecewise', None, 'peak', 'reflect', True),
+        ('c2', 150, 'morlet13.4', 'log', 'log', 'maximal', 'zero', True),
+        ('c3', 100, 'gmw3_60', 'linear', 'linear', 'energy', 'reflect', False),
+        ('c4', 200, 'morlet6', 'log:maximal', 'log', 'peak', 'reflect', True),
+    ]
+    for name, N, wk, st, sqf, mr, pad, flip in cases:
+        x = chirp_signal(N, seed=len(name) * 7 + N)
+        w = W(wk)
+        Tx, Wx, ssq_freqs, scales, wph, dWx = sq.ssq_cwt(
+            x, w, scales=st, nv=32, ssq_freqs=sqf, maprange=mr, padtype=pad,
+            flipud=flip, get_w=True, get_dWx=True)
+        Tx2, *_ = sq.ssq_cwt(x, w, scales=st, nv=32, ssq_freqs=sqf,
+                             maprange=mr, padtype=pad, flipud=flip)
+        assert np.allclose(Tx, Tx2, atol=1e-12)
+        tr[f'{name}/x'] = x
+        tr[f'{name}/meta'] = np.array([N, 32], dtype=np.int64)
+        tr[f'{name}/cfg'] = np.array([wk, st, str(sqf), mr, pad, str(flip)])
+        tr[f'{name}/Tx'] = Tx2
+        tr[f'{name}/Wx'] = Wx
+        if name == 'c0':
+            tr[f'{name}/w'] = wph
+        tr[f'{name}/ssq_freqs'] = np.asarray(ssq_freqs)
+        tr[f'{name}/scales'] = np.asarray(scales).ravel()
+        tr[f'{name}/icwt'] = sq.icwt(Wx, w, scales=scales, x_mean=x.mean())
+    # batched (equal length), matches looped per the reference tests
+    xb = np.stack([chirp_signal(100, seed=s) for s in (11, 12)])
+    w = W('morlet6')
+    Tx, Wx, f, s = sq.ssq_cwt(xb, w, scales='log-piecewise', nv=32,
+                              ssq_freqs='log')
+    tr['b0/x'], tr['b0/Tx'], tr['b0/Wx'] = xb, Tx, Wx
+    tr['b0/ssq_freqs'], tr['b0/scales'] = np.asarray(f), np.asarray(s).ravel()
+
+    # STFT
+    stft_cases = [('s0', 512, 'hann', 128, 128, 1),
+                  ('s1', 300, 'hann', 64, 48, 1),
+                  ('s2', 256, None, 64, 64, 1),
+                  ('s3', 400, 'hann', 64, 64, 3)]
+    for name, N, win, n_fft, win_len, hop in stft_cases:
+        x = chirp_signal(N, seed=N + 3)
+        Tx, Sx, ssq_freqs, Sfs, wph, dSx = sq.ssq_stft(
+            x, window=win, n_fft=n_fft, win_len=win_len, hop_len=hop,
+            dtype='float64', get_w=True, get_dWx=True)
+        Tx2, *_ = sq.ssq_stft(x, window=win, n_fft=n_fft, win_len=win_len,
+                              hop_len=hop, dtype='float64')
+        tr[f'{name}/x'] = x
+        tr[f'{name}/cfg'] = np.array([str(win), n_fft, win_len, hop])
+        tr[f'{name}/Tx'], tr[f'{name}/Sx'] = Tx2, Sx
+        if name == 's0':
+            tr[f'{name}/w'] = wph
+        tr[f'{name}/Sfs'] = np.asarray(Sfs)
+    np.savez_compressed(os.path.join(HERE, 'transforms.npz'), **tr)
+    print('transforms', len(tr))
+
+    #### full-size digests ####################################################
+    dg = {}
+    for name, N, wk, sqf in (('d10k', 10000, 'morlet6', 'log'),
+                             ('d160k', 160000, 'gmw3_60', None)):
+        x = chirp_signal(N, seed=0)
+        w = W(wk)
+        Tx, Wx, ssq_freqs, scales, wph = sq.ssq_cwt(
+            x, w, scales='log-piecewise', nv=32, ssq_freqs=sqf, get_w=True)
+        dg[f'{name}/Wx_rownorm'] = np.linalg.norm(Wx, axis=1)
+        dg[f'{name}/Wx_rowsum'] = Wx.sum(axis=1)
+        dg[f'{name}/Tx_rownorm'] = np.linalg.norm(Tx, axis=1)
+        dg[f'{name}/Tx_rowsum'] = Tx.sum(axis=1)
+        dg[f'{name}/Tx_colsum_stride'] = Tx.sum(axis=0)[::97]
+        dg[f'{name}/Wx_row'] = Wx[len(Wx) // 3][::16]
+        dg[f'{name}/Tx_row'] = Tx[np.argmax(np.linalg.norm(Tx, axis=1))][::16]
+        dg[f'{name}/Tx_row_idx'] = np.array(np.argmax(np.linalg.norm(Tx, axis=1)))
+        dg[f'{name}/ssq_freqs'] = np.asarray(ssq_freqs)
+        dg[f'{name}/scales'] = np.asarray(scales).ravel()
+        fin = np.isfinite(wph)
+        dg[f'{name}/w_finite'] = np.array(fin.sum())
+        dg[f'{name}/w_sum'] = np.array(wph[fin].sum())
+        print(name, Tx.shape)
+    np.savez_compressed(os.path.join(HERE, 'digests.npz'), **dg)
+
+
+if __name__ == '__main__':
+    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')

@@ -1,0 +1,100 @@
+# -*- coding: utf-8 -*-
+"""Pin the float64 oracle (oracle/ssq_oracle.py) against ssqueezepy's own
+float64 outputs stored in tests/golden/ (generated by make_golden.py)."""
+import numpy as np
+import pytest
+
+from oracle import ssq_oracle as O
+from ssqueezepy_b200 import _params as P
+from tests._cases import WAVS, CWT_CASES, STFT_CASES, oracle_kind, rel_l2, chirp_signal
+
+
+def _cwt_case(g, name):
+    wk, st, sqf, mr, pad, flip = [str(v) for v in g[f'{name}/cfg']]
+    x = g[f'{name}/x']
+    scales = g[f'{name}/scales']
+    ssq_freqs = g[f'{name}/ssq_freqs'][::-1]  # ascending, as squeezed
+    _, scaletype, _, nv = P.process_scales(scales, len(x), get_params=True)
+    const = P.squeeze_weights(scales, scaletype, nv, 'cwt')
+    sqtype = scaletype if sqf == 'None' else sqf
+    return dict(x=x, kind=oracle_kind(wk), scales=scales, ssq_freqs=ssq_freqs,
+                const=const, pad=pad, flip=(flip == 'True'),
+                logscale=sqtype.startswith('log'), scaletype=scaletype, nv=nv,
+                wk=wk)
+
+
+@pytest.mark.parametrize('name', CWT_CASES)
+def test_oracle_ssq_cwt_matches_reference(golden_transforms, name):
+    g = golden_transforms
+    c = _cwt_case(g, name)
+    Tx, Wx, w = O.ssq_cwt(c['x'], *c['kind'], c['scales'], c['ssq_freqs'],
+                          c['const'], padtype=c['pad'], logscale=c['logscale'],
+                          flipud=c['flip'])
+    assert rel_l2(Wx, g[f'{name}/Wx']) < 1e-13
+    assert rel_l2(Tx, g[f'{name}/Tx']) < 1e-12
+    if f'{name}/w' in g:
+        wr = g[f'{name}/w']
+        fin = np.isfinite(wr)
+        assert np.array_equal(fin, np.isfinite(w))
+        assert np.allclose(w[fin], wr[fin], rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize('name', CWT_CASES)
+def test_oracle_icwt_matches_reference(golden_transforms, name):
+    g = golden_transforms
+    c = _cwt_case(g, name)
+    wav = P.Wavelet((WAVS[c['wk']][0], dict(WAVS[c['wk']][1], dtype='float64')))
+    Cpsi = P.adm_ssq(wav)
+    x = O.icwt(g[f'{name}/Wx'], c['scales'], c['scaletype'], c['nv'], Cpsi,
+               x_mean=c['x'].mean())
+    assert np.allclose(x, g[f'{name}/icwt'], rtol=1e-12, atol=1e-12)
+
+
+def test_oracle_batched_matches_reference(golden_transforms):
+    g = golden_transforms
+    x, scales = g['b0/x'], g['b0/scales']
+    _, st, _, nv = P.process_scales(scales, x.shape[-1], get_params=True)
+    const = P.squeeze_weights(scales, st, nv, 'cwt')
+    Tx, Wx, _ = O.ssq_cwt(x, 'morlet', (6.,), scales, g['b0/ssq_freqs'][::-1],
+                          const)
+    assert rel_l2(Wx, g['b0/Wx']) < 1e-13
+    assert rel_l2(Tx, g['b0/Tx']) < 1e-12
+
+
+@pytest.mark.parametrize('name', STFT_CASES)
+def test_oracle_ssq_stft_matches_reference(golden_transforms, name):
+    g = golden_transforms
+    win, n_fft, win_len, hop = [str(v) for v in g[f'{name}/cfg']]
+    n_fft, win_len, hop = int(n_fft), int(win_len), int(hop)
+    window, dwin = P.get_window(None if win == 'None' else win, win_len,
+                                n_fft, derivative=True)
+    Tx, Sx, w, Sfs = O.ssq_stft(g[f'{name}/x'], window, dwin, n_fft, hop)
+    assert rel_l2(Sx, g[f'{name}/Sx']) < 1e-13
+    assert rel_l2(Tx, g[f'{name}/Tx']) < 1e-12
+    assert np.allclose(Sfs, g[f'{name}/Sfs'])
+    if f'{name}/w' in g:
+        wr = g[f'{name}/w']
+        fin = np.isfinite(wr)
+        assert np.array_equal(fin, np.isfinite(w))
+        assert np.allclose(w[fin], wr[fin], rtol=1e-9, atol=1e-12)
+
+
+def test_oracle_full_size_digest_10k(golden_digests):
+    """N=10,000 chirp, Morlet mu=6, log-piecewise scales, log ssq_freqs."""
+    d = golden_digests
+    x = chirp_signal(10000, seed=0)
+    scales = d['d10k/scales']
+    _, st, _, nv = P.process_scales(scales, 10000, get_params=True)
+    const = P.squeeze_weights(scales, st, nv, 'cwt')
+    Tx, Wx, w = O.ssq_cwt(x, 'morlet', (6.,), scales, d['d10k/ssq_freqs'][::-1],
+                          const)
+    assert np.allclose(np.linalg.norm(Wx, axis=1), d['d10k/Wx_rownorm'],
+                       rtol=1e-11)
+    assert np.allclose(Wx.sum(1), d['d10k/Wx_rowsum'], rtol=1e-9, atol=1e-9)
+    assert np.allclose(np.linalg.norm(Tx, axis=1), d['d10k/Tx_rownorm'],
+                       rtol=1e-9, atol=1e-12)
+    assert np.allclose(Tx.sum(1), d['d10k/Tx_rowsum'], rtol=1e-9, atol=1e-9)
+    r = int(d['d10k/Tx_row_idx'])
+    assert np.allclose(Tx[r][::16], d['d10k/Tx_row'], rtol=1e-9, atol=1e-12)
+    fin = np.isfinite(w)
+    assert fin.sum() == int(d['d10k/w_finite'])
