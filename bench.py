@@ -1,0 +1,310 @@
+# -*- coding: utf-8 -*-
+"""Benchmark of the synchrosqueezing hot path: ssq_cwt forward, float32,
+one N=160,000 signal per GPU per step (linear chirp 0.01->0.2 cycles/sample +
+AM tone at 0.3 + N(0, 0.1^2) noise), GMW gamma=3 beta=60, nv=32,
+log-piecewise scales (293 rows), reflect padding (Npad = 262,144).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` is signal-samples/s over all ranks with
+inputs resident in HBM and outputs preallocated (the C-ABI calls of one
+ssq_cwt: fused CWT + squeeze); `e2e` is the same metric through the public
+`ssq_cwt` call from pinned host memory, including the host->device copy of x
+and the device->host copy of Tx. Each rank processes its own signal (weak
+scaling, no collective on the data path). `--impl reference` times the CPU
+restatement of ssqueezepy's algorithm (oracle/ssq_oracle.py, float64, all
+host threads) on the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("ssq_cwt signal-samples/s fwd & fwd+bwd, batched vs plain, "
+          "% of HBM roofline")
+UNIT = "signal-samples/s"
+N_SIG = 160000
+WAVELET = ('gmw', {'gamma': 3., 'beta': 60., 'dtype': 'float32'})
+L2_BYTES = 126 * 2**20
+
+
+def chirp_signal(N, seed=0):
+    t = np.arange(N, dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    return (np.cos(2 * np.pi * (0.01 * t + 0.19 * t**2 / (2 * N)))
+            + (0.5 + 0.5 * np.cos(2 * np.pi * 0.001 * t))
+            * np.cos(2 * np.pi * 0.3 * t)
+            + 0.1 * rng.standard_normal(N))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            d = json.load(f)
+        return float(d['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.rows, self.proc = [], None
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '--query-gpu=' + self.Q, '--format=csv,noheader,nounits',
+                 '-lms', '200', '-i', str(gpu_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(',')])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == 'active':
+                        reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def oracle_step(x, scales, f_asc, const):
+    from oracle import ssq_oracle as O
+    return O.ssq_cwt(x, 'gmw_l1', (3., 60.), scales, f_asc, const)
+
+
+def host_params():
+    from ssqueezepy_b200 import _params as P
+    w = P.Wavelet(WAVELET)
+    sc, st, na, nv = P.process_scales('log-piecewise', N_SIG, w, nv=32,
+                                      get_params=True)
+    f = P.compute_associated_frequencies(sc, N_SIG, w, st, 'peak', True, 1., 'cwt')
+    const = P.squeeze_weights(sc, st, nv, 'cwt')
+    return w, sc.ravel(), f, const, na
+
+
+def run_reference(args):
+    rank = int(os.environ.get('RANK', 0))
+    if rank != 0:
+        return 0
+    w, sc, f, const, na = host_params()
+    x = chirp_signal(N_SIG, seed=0)
+    for _ in range(args.warmup):
+        oracle_step(x, sc, f, const)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle_step(x, sc, f, const)
+    dt = time.perf_counter() - t0
+    v = args.steps * N_SIG / dt
+    cores = os.cpu_count()
+    sample = ("full workload per step: one N=160,000 signal, float64 numpy/scipy "
+              "restatement, scipy.fft workers=%d" % cores)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "ssq_cwt N=160000 GMW(3,60) nv=32 log-piecewise "
+                                   "(293 rows) float32 reflect",
+                       "N": N_SIG, "na": na, "parallelism": "rank0 CPU"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import ssqueezepy_b200 as sb
+    from ssqueezepy_b200 import _lib as L
+    from ssqueezepy_b200 import _params as P
+
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    rank = int(os.environ.get('RANK', 0))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    lib = L.load()
+    w, sc, f, const, na = host_params()
+    N = N_SIG
+    Npad, n1, _ = P.p2up(N)
+    x_np = chirp_signal(N, seed=rank).astype(np.float32)
+    x = torch.as_tensor(x_np, device=dev)
+    Wx = torch.empty((1, na, N), dtype=torch.complex64, device=dev)
+    Tx = torch.empty_like(Wx)
+    idx = torch.empty((1, na, N), dtype=torch.uint16, device=dev)
+    wsb = lib.ssqb_cwt_workspace_bytes(1, N, Npad, na, L.F32)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    sc_d = torch.as_tensor(sc, dtype=torch.float64, device=dev)
+    cst_d = torch.as_tensor(const, dtype=torch.float64, device=dev)
+    kind, *wp = w.kernel_params()
+    cw = L.make_wavelet(kind, wp)
+    mode, bp = P.bin_params(f, True)
+    cb = L.make_bins(mode, bp, na, True)
+    gamma = 10 * P.EPS32
+    st = torch.cuda.current_stream()
+    sp = L.stream_ptr(st)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    launches = lib.ssqb_cwt_launches(1, Npad, na, L.F32, wsb) + 1
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(st)
+        L.check(lib.ssqb_cwt(L.ptr(x), 1, N, Npad, n1, 1, 0, L.ptr(sc_d), na, cw, 1.0,
+                             cb, gamma, L.F32, L.ptr(Wx), None, None, L.ptr(idx),
+                             L.ptr(ws), wsb, sp), 'cwt')
+        if ev:
+            ev[1].record(st)
+        L.check(lib.ssqb_squeeze(L.ptr(Wx), L.ptr(idx), L.ptr(cst_d), 1, na, N, na,
+                                 L.F32, L.ptr(Tx), sp), 'squeeze')
+        if ev:
+            ev[2].record(st)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    assert L.device_status() == 0
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)]
+           for _ in range(args.steps)]
+    clk = Clocks(local) if rank == 0 else None
+    barrier()
+    for k in range(args.steps):
+        flush.zero_()  # write 252 MB > L2 between timed steps (outside events)
+        step(evs[k])
+    barrier()
+    clocks = clk.stop() if clk else None
+    cwt_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    sq_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    step_ms = float(np.sum(cwt_ms) + np.sum(sq_ms)) / args.steps
+    t_local = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    step_ms_max = float(t_local.item())
+    value = world * N / (step_ms_max * 1e-3)
+
+    # end to end through the public API from pinned host memory
+    x_pin = torch.from_numpy(x_np).pin_memory()
+    Tx_pin = torch.empty((na, N), dtype=torch.complex64).pin_memory()
+    for _ in range(2):
+        Tp, *_ = sb.ssq_cwt(x_pin, WAVELET, scales='log-piecewise', nv=32)
+        Tx_pin.copy_(Tp, non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, min(args.steps, 10))
+    e0.record(st)
+    for _ in range(e2e_steps):
+        Tp, *_ = sb.ssq_cwt(x_pin, WAVELET, scales='log-piecewise', nv=32)
+        Tx_pin.copy_(Tp, non_blocking=True)
+    e1.record(st)
+    barrier()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1) / e2e_steps], dtype=torch.float64,
+                          device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_value = world * N / (float(e2e_ms.item()) * 1e-3)
+
+    if rank == 0:
+        hbm, src = peaks()
+        alg_cwt = (4 + 8 * na) * N          # read x, write Wx
+        alg_total = (4 + 16 * na) * N       # read x, write Wx and Tx
+        cwt_avg = float(np.mean(cwt_ms))
+        sq_avg = float(np.mean(sq_ms))
+        dom, dom_ms, dom_bytes = (('cwt', cwt_avg, alg_cwt) if cwt_avg >= sq_avg else
+                                  ('squeeze', sq_avg, 8 * na * N))
+        achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ssq_cwt N=160000 GMW(3,60) nv=32 log-piecewise "
+                                   "(293 rows) float32 reflect, one signal per GPU",
+                       "N": N, "na": na, "Npad": Npad, "batch_per_gpu": 1,
+                       "l2": "252 MB buffer written between timed steps",
+                       "parallelism": "dp%d" % world},
+            "stages_ms": {"cwt": cwt_avg, "squeeze": sq_avg},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "peak_source": src,
+                         "path_frac": alg_total / (step_ms_max * 1e-3) / 1e9 / hbm},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * N,
+                    "d2h_bytes_per_step": 8 * na * N},
+            "gpu_launches": launches * args.steps,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu:
+            t0 = time.perf_counter()
+            To, Wo, _ = oracle_step(chirp_signal(N, seed=0), sc, f, const)
+            tc = time.perf_counter() - t0
+            line["cpu_baseline"] = {
+                "value": N / tc, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                "sample": "one full N=160,000 ssq_cwt, float64 numpy/scipy restatement"}
+            Tg, Wg = Tx[0].cpu().numpy(), Wx[0].cpu().numpy()
+            line["parity"] = {
+                "Wx_rel_l2": float(np.linalg.norm(Wg - Wo) / np.linalg.norm(Wo)),
+                "Tx_rel_l2": float(np.linalg.norm(Tg - To) / np.linalg.norm(To))}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--no-cpu', action='store_true',
+                    help='skip the CPU baseline / parity leg')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == '__main__':
+    sys.exit(main())

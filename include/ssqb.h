@@ -1,0 +1,156 @@
+/* ssqb: B200-native (sm_100a) synchrosqueezing hot path, C ABI.
+ *
+ * Every entry point takes device pointers, sizes and a CUDA stream
+ * (`stream`, a cudaStream_t passed as void*, NULL = legacy default stream),
+ * returns an int status (SSQB_OK = 0) and allocates nothing: outputs and
+ * workspaces belong to the caller. Work is enqueued on `stream`; calls return
+ * before it completes. Layouts are C-contiguous; complex arrays are
+ * interleaved (re, im) pairs of float (SSQB_F32) or double (SSQB_F64).
+ *
+ * Shapes: B signals of N samples each; na rows (CWT scales or STFT
+ * frequencies); nbins rows of Tx (= na for the transforms here).
+ *
+ * The entry points replace the GPU seams of ssqueezepy (paths are relative
+ * to its source tree):
+ *   ssqb_cwt            _cwt.py:250-311 (pad, fft, Psih*xh, two ifft,
+ *                       unpad) + algos.py:743-781 (phase_cwt_gpu) fused,
+ *                       and the bin search of algos.py:1008-1128
+ *   ssqb_squeeze        utils/gpu_utils.py:10-14 launching the
+ *                       `ssq_cwt_*` / `ssq_stft` kernels of
+ *                       algos.py:1007-1167 (here reading a bin index)
+ *   ssqb_ssqueeze_fast  algos.py:126-150 (ssqueeze_fast) on the GPU
+ *   ssqb_indexed_sum    algos.py:153-169 (indexed_sum_onfly) on the GPU
+ *   ssqb_stft           _stft.py:127-181 + utils/stft_utils.py:101-138
+ *                       (buffer) + algos.py:818-856 (phase_stft_gpu) fused
+ */
+#ifndef SSQB_H_
+#define SSQB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SSQB_API __attribute__((visibility("default")))
+#else
+#define SSQB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SSQB_OK = 0,
+  SSQB_EINVAL = 1,        /* bad argument (message in ssqb_last_error) */
+  SSQB_EUNSUPPORTED = 2,  /* valid but not supported (e.g. non power-of-2 length) */
+  SSQB_ECUDA = 3,         /* CUDA runtime error */
+  SSQB_EWORKSPACE = 4     /* workspace smaller than required */
+};
+
+enum { SSQB_F32 = 0, SSQB_F64 = 1 };
+
+/* padtype: 0 zero, 1 reflect, 2 symmetric, 3 replicate, 4 wrap
+ * (utils/common.py:54-158) */
+
+/* Frequency-domain wavelet (wavelets.py:498-530, _gmw.py:187-251).
+ * kind 0 Morlet:   p = {mu, ks = exp(-mu^2/2), C1 = sqrt(2) cs pi^(1/4), 0}
+ * kind 1 GMW L1:   p = {gamma, beta, wc = (beta/gamma)^(1/gamma), log(wc)}
+ * kind 2 GMW L2:   p = {gamma, beta, wc, sqrt(2 pi gamma 2^r / Gamma(r))} */
+typedef struct ssqb_wavelet {
+  int32_t kind;
+  int32_t reserved;
+  double p[4];
+} ssqb_wavelet;
+
+/* Bin mapping of the squeeze (algos.py:81-87, 356-374).
+ * mode 0 log:           p = {vlmin, dvl}
+ * mode 1 log-piecewise: p = {vlmin0, vlmin1, dvl0, dvl1}, idx1
+ * mode 2 linear:        p = {vmin, dv}
+ * flipud: k -> nbins-1-k (ssqueezing.py:13-15, algos.py:95) */
+typedef struct ssqb_bins {
+  int32_t mode;
+  int32_t idx1;
+  int32_t flipud;
+  int32_t nbins;
+  double p[4];
+} ssqb_bins;
+
+SSQB_API int ssqb_version(void);
+
+/* Message of the last failing call on this host thread. */
+SSQB_API const char* ssqb_last_error(void);
+
+/* Copy and clear the device status word of the current device (0 = ok,
+ * 1 = bin index out of range, 2 = padded index out of range); synchronizes
+ * `stream`. */
+SSQB_API int ssqb_device_status(void* stream, int* status_out);
+
+/* Workspace bytes for ssqb_cwt: the float64 padded-signal spectrum plus
+ * the two-pass intermediate for a tile of rows (sized to stay in L2). */
+SSQB_API size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision);
+
+/* Number of kernel launches one ssqb_cwt call makes with this workspace
+ * size (padded-signal FFT plus CWT passes); no reference counterpart. */
+SSQB_API int ssqb_cwt_launches(int B, int Npad, int na, int precision,
+                               size_t workspace_bytes);
+
+/* Fused CWT (replaces _cwt.py:250-311 with derivative=True, l1_norm=True,
+ * plus the phase transform and bin search of algos.py:859-953):
+ *   x      (B, N) float (F32) or double (F64)
+ *   scales (na) double, device
+ *   Wx     (B, na, N) complex, required; dWx optional (NULL)
+ *   w      (B, na, N) real phase transform, optional (inf where |Wx|<gamma)
+ *   idx    (B, na, N) uint16 bin of each entry, 0xFFFF where |Wx|<=gamma;
+ *          optional (needs `bins`)
+ * Npad is the padded length (a power of two, 8 <= Npad <= 2^22) and n1 the
+ * left pad; dt = 1/fs. rpadded != 0 writes all Npad columns (outputs
+ * (B, na, Npad), _cwt.py:293-306 with rpadded=True). */
+SSQB_API int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
+             const double* scales, int na, const ssqb_wavelet* wavelet, double dt,
+             const ssqb_bins* bins, double gamma, int precision,
+             void* Wx, void* dWx, void* w, uint16_t* idx,
+             void* workspace, size_t workspace_bytes, void* stream);
+
+/* Squeeze from a bin index: Tx[b, idx, j] += Wx[b, i, j] * row_weights[i]
+ * over i ascending (algos.py:859-984 accumulation order). Tx (B, nbins, N)
+ * is overwritten. */
+SSQB_API int ssqb_squeeze(const void* Wx, const uint16_t* idx, const double* row_weights,
+                 int B, int na, int N, int nbins, int precision, void* Tx,
+                 void* stream);
+
+/* Squeeze computing the phase transform on the fly from Wx and dWx
+ * (ssqueeze_fast, algos.py:126-150). Sfs (na) non-NULL selects the STFT
+ * phase transform |Sfs_i - Im(dS/S)/2pi| (algos.py:956-984). */
+SSQB_API int ssqb_ssqueeze_fast(const void* Wx, const void* dWx, const double* Sfs,
+                       const double* row_weights, const ssqb_bins* bins, double gamma,
+                       int B, int na, int N, int precision, void* Tx, void* stream);
+
+/* Squeeze from a precomputed phase transform w (inf = skip)
+ * (indexed_sum_onfly, algos.py:153-250). */
+SSQB_API int ssqb_indexed_sum(const void* Wx, const void* w, const double* row_weights,
+                     const ssqb_bins* bins, int B, int na, int N, int precision,
+                     void* Tx, void* stream);
+
+/* Fused STFT (replaces _stft.py:127-181 with derivative=True and the
+ * phase transform of algos.py:784-816): x (B, N); window and diff_window
+ * (n_fft) double, diff_window already scaled as the reference does (times
+ * fs when modulated); Sfs (n_fft/2+1) double. Outputs (B, n_fft/2+1,
+ * n_frames), n_frames = (N-1)/hop + 1; dSx, w, idx optional. n_fft is a
+ * power of two <= 4096; n1 is the left pad of the N + n_fft - 1 padding. */
+SSQB_API int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padtype,
+              int modulated, const double* window, const double* diff_window,
+              const double* Sfs, const ssqb_bins* bins, double gamma, int precision,
+              void* Sx, void* dSx, void* w, uint16_t* idx, void* stream);
+
+/* One-integral inverse CWT as a weighted row sum (_cwt.py:479-482 with the
+ * scaling of :441-452): x[b, j] = sum_i Re(Wx[b, i, j]) * row_weights[i]
+ * + x_mean[b] * mean_weight. x (B, N) real of the given precision; x_mean
+ * (B) double, may be NULL. */
+SSQB_API int ssqb_icwt(const void* Wx, const double* row_weights, const double* x_mean,
+                       double mean_weight, int B, int na, int N, int precision,
+                       void* x, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SSQB_H_ */

@@ -1,3 +1,25 @@
 # -*- coding: utf-8 -*-
-"""B200-native synchrosqueezing hot path (ssq_cwt / cwt / ssq_stft / stft /
-icwt) with ssqueezepy's signatures and return tuples."""
+"""B200-native synchrosqueezing hot path.
+
+Drop-in replacements for ssqueezepy's `ssq_cwt`, `cwt`, `icwt`, `ssq_stft`,
+`stft` and `ssqueeze` (same signatures and return tuples), computed by the
+hand-written sm_100a CUDA kernels of `_lib/libssqb.so` (C ABI:
+include/ssqb.h). Host code only derives float64 parameters (scales,
+frequencies, bin mapping); there is no CPU fallback.
+"""
+from ._transforms import (cwt, ssq_cwt, icwt, stft, ssq_stft, ssqueeze,
+                          phase_cwt, phase_stft, Wavelet)
+from ._params import (p2up, process_scales, make_scales, cwt_scalebounds,
+                      center_frequency, adm_ssq, logscale_transition_idx,
+                      infer_scaletype, nv_from_scales)
+from . import _lib
+
+__version__ = '0.1.0'
+__all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
+           'phase_cwt', 'phase_stft', 'Wavelet', 'p2up', 'process_scales',
+           'make_scales', 'cwt_scalebounds', 'center_frequency', 'adm_ssq',
+           'logscale_transition_idx', 'infer_scaletype', 'nv_from_scales']
+
+
+def wavs():
+    return Wavelet.SUPPORTED

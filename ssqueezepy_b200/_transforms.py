@@ -1,0 +1,594 @@
+# -*- coding: utf-8 -*-
+"""Drop-in `cwt`, `ssq_cwt`, `icwt`, `stft`, `ssq_stft`, `ssqueeze` on the
+GPU. Signatures and return tuples follow ssqueezepy (paths relative to its
+source tree): `ssq_cwt` _ssq_cwt.py:12-310, `cwt` _cwt.py:12-320, `icwt`
+_cwt.py:323-453, `stft` _stft.py:13-181, `ssq_stft` _ssq_stft.py:13-136,
+`ssqueeze` ssqueezing.py:13-224.
+
+Host work is the float64 parameter math of `_params`; every array operation
+runs in the CUDA kernels of libssqb.so (through `_lib`). Inputs may be numpy
+arrays or torch tensors (CPU or CUDA); outputs are CUDA tensors
+(`astensor=True`, the default) or numpy arrays.
+"""
+import numpy as np
+import torch
+
+from . import _lib as L
+from . import _params as P
+
+__all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
+           'phase_cwt', 'phase_stft', 'Wavelet']
+
+Wavelet = P.Wavelet
+
+_CDT = {'float32': torch.complex64, 'float64': torch.complex128}
+_RDT = {'float32': torch.float32, 'float64': torch.float64}
+
+
+#### helpers #################################################################
+def _device_of(x):
+    if isinstance(x, torch.Tensor) and x.is_cuda:
+        return x.device
+    return torch.device('cuda', torch.cuda.current_device())
+
+
+def _to_device(x, dtype, nan_checks):
+    """(B, N) contiguous CUDA tensor of `dtype` and whether x was 2D."""
+    if not hasattr(x, 'ndim'):
+        raise TypeError("`x` must be a numpy array or torch Tensor "
+                        "(got %s)" % type(x))
+    if x.ndim not in (1, 2):
+        raise ValueError("`x` must be 1D or 2D (got x.ndim == %s)" % x.ndim)
+    L.require_cuda()
+    is_np = isinstance(x, np.ndarray)
+    if nan_checks is None:
+        nan_checks = is_np
+    if nan_checks:
+        if not is_np:
+            raise ValueError("`nan_checks=True` requires NumPy input.")
+        if not np.isfinite(x).all():  # _cwt.py:208-215 zeroes NaN / inf
+            x = np.where(np.isfinite(x), x, 0)
+    dev = _device_of(x)
+    t = torch.as_tensor(x)
+    t = t.to(device=dev, dtype=_RDT[dtype], non_blocking=True)
+    is_2d = t.ndim == 2
+    return t.reshape(-1, t.shape[-1]).contiguous(), is_2d
+
+
+def _out(t, astensor, is_2d=True):
+    if t is None:
+        return None
+    if not is_2d and t.ndim >= 1 and t.shape[0] == 1:
+        t = t[0]
+    if astensor:
+        return t
+    return t.cpu().numpy()
+
+
+def _prec(dtype):
+    return L.F64 if dtype == 'float64' else L.F32
+
+
+def _default_gamma(dtype):
+    return 10 * (P.EPS64 if dtype == 'float64' else P.EPS32)
+
+
+def _dev_f64(a, dev):
+    return torch.as_tensor(np.ascontiguousarray(np.asarray(a, np.float64).ravel()),
+                           device=dev)
+
+
+#### host parameter cache ###################################################
+# The scale and frequency searches cost milliseconds of host time; a given
+# (wavelet, N, scheme) always yields the same float64 parameters, so they are
+# computed once. Device copies are kept per device.
+_PLANS = {}
+_PLAN_MAX = 64
+
+
+def _wkey(wavelet):
+    return (wavelet.name_, tuple(sorted(wavelet.config.items())), wavelet.dtype)
+
+
+def _akey(a):
+    if a is None or isinstance(a, (str, int, float, tuple)):
+        return a
+    a = np.ascontiguousarray(P._to_numpy(a))
+    return (a.dtype.str, a.shape, a.tobytes())
+
+
+def _plan(key, make):
+    p = _PLANS.get(key)
+    if p is None:
+        if len(_PLANS) >= _PLAN_MAX:
+            _PLANS.pop(next(iter(_PLANS)))
+        p = _PLANS[key] = make()
+        p['dev'] = {}
+    return p
+
+
+def _on_device(plan, name, dev):
+    k = (name, str(dev))
+    t = plan['dev'].get(k)
+    if t is None:
+        t = plan['dev'][k] = _dev_f64(plan[name], dev)
+    return t
+
+
+def _scales_plan(scales, N, wavelet, nv):
+    def make():
+        if isinstance(scales, str):
+            sc, st, na, nv_ = P.process_scales(scales, N, wavelet, nv=nv,
+                                               get_params=True)
+        else:
+            sc, st, na, nv_ = P.process_scales(P._to_numpy(scales), N,
+                                               get_params=True)
+        return dict(scales=np.asarray(sc, np.float64).ravel(), scaletype=st,
+                    na=na, nv=nv_)
+    return _plan(('scales', _wkey(wavelet), N, _akey(scales), nv), make)
+
+
+#### CWT #####################################################################
+def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
+              derivative, want_idx=False, want_w=False, ssq=None, gamma=None):
+    """Run the fused CWT kernel. Returns dict of device tensors + params."""
+    N = x.shape[-1]
+    dt, fs, _ = P.process_fs_and_t(fs, t, N)
+    wavelet = P.Wavelet._init_if_not_isinstance(wavelet)
+    dtype = wavelet.dtype
+    xd, is_2d = _to_device(x, dtype, nan_checks)
+    dev = xd.device
+    sp = _scales_plan(scales, N, wavelet, nv)
+    scales_np, scaletype, na, nv = sp['scales'], sp['scaletype'], sp['na'], sp['nv']
+    if padtype is None:
+        Npad, n1 = N, 0
+        if Npad & (Npad - 1):
+            raise NotImplementedError("`padtype=None` needs a power-of-2 length "
+                                      "on the accelerated path")
+        ptype = 5
+    else:
+        if padtype not in L.PADTYPES:
+            raise ValueError("`padtype` must be one of %s (got %s)"
+                             % (list(L.PADTYPES), padtype))
+        Npad, n1, _ = P.p2up(N)
+        ptype = L.PADTYPES[padtype]
+    B = xd.shape[0]
+    ncol = Npad if (rpadded and padtype is not None) else N
+    prec = _prec(dtype)
+    cdt, rdt = _CDT[dtype], _RDT[dtype]
+    Wx = torch.empty((B, na, ncol), dtype=cdt, device=dev)
+    dWx = torch.empty_like(Wx) if derivative else None
+    w = torch.empty((B, na, ncol), dtype=rdt, device=dev) if want_w else None
+    idx = (torch.empty((B, na, ncol), dtype=torch.uint16, device=dev)
+           if want_idx else None)
+    wsb = L.load().ssqb_cwt_workspace_bytes(B, N, Npad, na, prec)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    sc_d = _on_device(sp, 'scales', dev)
+    kind, *wp = wavelet.kernel_params()
+    cw = L.make_wavelet(kind, wp)
+    cb = L.make_bins(*ssq) if ssq is not None else None
+    gamma = _default_gamma(dtype) if gamma is None else gamma
+    with torch.cuda.device(dev):
+        rc = L.load().ssqb_cwt(
+            L.ptr(xd), B, N, Npad, n1, ptype, 1 if (rpadded and padtype) else 0,
+            L.ptr(sc_d), na, cw, float(dt), cb, float(gamma), prec,
+            L.ptr(Wx), L.ptr(dWx), L.ptr(w), L.ptr(idx), L.ptr(ws), wsb,
+            L.stream_ptr())
+    L.check(rc, 'cwt')
+    return dict(Wx=Wx, dWx=dWx, w=w, idx=idx, scales=scales_np,
+                scaletype=scaletype, nv=nv, na=na, N=N, dt=dt, fs=fs,
+                wavelet=wavelet, dtype=dtype, is_2d=is_2d, dev=dev, B=B,
+                gamma=gamma, sc_d=sc_d)
+
+
+def cwt(x, wavelet='gmw', scales='log-piecewise', fs=None, t=None, nv=32,
+        l1_norm=True, derivative=False, padtype='reflect', rpadded=False,
+        vectorized=True, astensor=True, cache_wavelet=None, order=0, average=None,
+        nan_checks=None, patience=0):
+    """Continuous Wavelet Transform; returns `(Wx, scales[, dWx])`
+    (_cwt.py:12-320). `vectorized`, `cache_wavelet` and `patience` only
+    select CPU strategies in the reference and have no effect here."""
+    if isinstance(order, (tuple, list, range)) or order > 0:
+        raise NotImplementedError("higher-order GMW `cwt` (order > 0) is not on "
+                                  "the accelerated path")
+    if not isinstance(scales, str):
+        nv = None
+    wavelet = P.process_gmw_wavelet(wavelet, l1_norm)
+    r = _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
+                  derivative)
+    Wx, dWx = r['Wx'], r['dWx']
+    if not l1_norm:
+        s = torch.as_tensor(np.sqrt(r['scales'].ravel()), device=r['dev'],
+                            dtype=_RDT[r['dtype']]).reshape(1, -1, 1)
+        Wx = Wx * s
+        dWx = dWx * s if dWx is not None else None
+    scales_out = _scales_out(r, astensor)
+    Wx, dWx = _out(Wx, astensor, r['is_2d']), _out(dWx, astensor, r['is_2d'])
+    return (Wx, scales_out, dWx) if derivative else (Wx, scales_out)
+
+
+def _scales_out(r, astensor):
+    s = r['scales'].ravel().astype(r['dtype'])
+    if astensor:
+        return torch.as_tensor(s, device=r['dev'])
+    return s
+
+
+def _check_ssq_args(squeezing, maprange, difftype):
+    if not isinstance(squeezing, str):
+        raise NotImplementedError("custom `squeezing` functions are not on the "
+                                  "accelerated path")
+    if squeezing not in ('sum', 'lebesgue', 'abs'):
+        raise ValueError("`squeezing` must be one of: sum, lebesgue, abs "
+                         "(got %s)" % squeezing)
+    if squeezing != 'sum':
+        raise NotImplementedError("only squeezing='sum' is on the accelerated "
+                                  "path")
+    if isinstance(maprange, (tuple, list)):
+        if not all(isinstance(m, (float, int)) for m in maprange):
+            raise ValueError("all elements of `maprange` must be float or int")
+    elif isinstance(maprange, str):
+        if maprange not in ('maximal', 'peak', 'energy'):
+            raise ValueError("`maprange` must be one of: maximal, peak, energy "
+                             "(got %s)" % maprange)
+    else:
+        raise TypeError("`maprange` must be str, tuple, or list "
+                        "(got %s)" % type(maprange))
+    if difftype not in ('trig', 'phase', 'numeric'):
+        raise ValueError("`difftype` must be one of: direct, phase, numeric"
+                         " (got %s)" % difftype)
+    if difftype != 'trig':
+        raise ValueError("GPU computation only supports `difftype = 'trig'`")
+
+
+def _ssq_freqs_for_cwt(ssq_freqs, scales, N, wavelet, cwt_scaletype, maprange,
+                       was_padded, dt):
+    """Ascending ssq_freqs (float64) and whether bins are log-spaced
+    (ssqueezing.py:168-194)."""
+    if isinstance(ssq_freqs, (np.ndarray, torch.Tensor)):
+        f = P._to_numpy(ssq_freqs).astype(np.float64).ravel()
+        st, _ = P.infer_scaletype(f)
+        return f, st.startswith('log')
+    st = ssq_freqs if isinstance(ssq_freqs, str) else cwt_scaletype
+    if ((maprange == 'maximal' or isinstance(maprange, tuple)) and
+            st == 'log-piecewise'):
+        raise ValueError("can't have `ssq_scaletype = log-piecewise` or "
+                         "tuple with `maprange = 'maximal'` "
+                         "(got %s)" % str(maprange))
+    f = P.compute_associated_frequencies(scales, N, wavelet, st, maprange,
+                                         was_padded, dt, 'cwt')
+    return np.asarray(f, np.float64), st.startswith('log')
+
+
+def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
+            ssq_freqs=None, padtype='reflect', squeezing='sum', maprange='peak',
+            difftype='trig', difforder=None, gamma=None, vectorized=True,
+            preserve_transform=None, astensor=True, order=0, nan_checks=None,
+            patience=0, flipud=True, cache_wavelet=None, get_w=False,
+            get_dWx=False):
+    """Synchrosqueezed CWT; returns `(Tx, Wx, ssq_freqs, scales[, w][, dWx])`
+    (_ssq_cwt.py:12-310). `ssq_freqs` comes back as a float64 numpy array,
+    high to low (ssqueezing.py:216-224)."""
+    if x.ndim == 2 and get_w:
+        raise NotImplementedError("`get_w=True` unsupported with batched input.")
+    _check_ssq_args(squeezing, maprange, difftype)
+    if isinstance(order, (tuple, list, range)) or order > 0:
+        raise NotImplementedError("higher-order GMW `ssq_cwt` (order > 0) is not "
+                                  "on the accelerated path")
+    if nv is None and not isinstance(scales, np.ndarray):
+        nv = 32
+    N = x.shape[-1]
+    dt, fs, _ = P.process_fs_and_t(fs, t, N)
+    wavelet = P.Wavelet._init_if_not_isinstance(wavelet, N=N)
+    sp = _scales_plan(scales, N, wavelet, nv)
+    sc, cwt_st, na, nv_ = sp['scales'], sp['scaletype'], sp['na'], sp['nv']
+
+    def make():
+        f_asc, logscale = _ssq_freqs_for_cwt(
+            ssq_freqs, sc.reshape(-1, 1), N, wavelet, cwt_st, maprange,
+            padtype is not None, dt)
+        mode, bp = P.bin_params(f_asc, logscale)
+        const = P.squeeze_weights(sc, cwt_st, nv_, 'cwt')
+        return dict(f_asc=f_asc, mode=mode, bp=bp, const=const)
+    fp = _plan(('ssq', _wkey(wavelet), N, _akey(scales), nv, _akey(ssq_freqs),
+                _akey(maprange), padtype is not None, dt), make)
+    f_asc = fp['f_asc']
+    r = _cwt_core(x, wavelet, scales, nv, fs, t, padtype, False, nan_checks,
+                  get_dWx, want_idx=True, want_w=get_w,
+                  ssq=(fp['mode'], fp['bp'], na, flipud), gamma=gamma)
+    Tx = torch.empty_like(r['Wx'])
+    cst = _on_device(fp, 'const', r['dev'])
+    with torch.cuda.device(r['dev']):
+        rc = L.load().ssqb_squeeze(L.ptr(r['Wx']), L.ptr(r['idx']), L.ptr(cst),
+                                   r['B'], na, N, na, _prec(r['dtype']),
+                                   L.ptr(Tx), L.stream_ptr())
+    L.check(rc, 'squeeze')
+    is2 = r['is_2d']
+    out = [_out(Tx, astensor, is2), _out(r['Wx'], astensor, is2), f_asc[::-1],
+           _scales_out(r, astensor)]
+    if get_w:
+        out.append(_out(r['w'], astensor, is2))
+    if get_dWx:
+        out.append(_out(r['dWx'], astensor, is2))
+    return tuple(out)
+
+
+def icwt(Wx, wavelet='gmw', scales='log-piecewise', nv=None, one_int=True,
+         x_len=None, x_mean=0, padtype='reflect', rpadded=False, l1_norm=True):
+    """One-integral inverse CWT (_cwt.py:323-453) as one weighted row sum on
+    the GPU. `Wx` (na, n) or (B, na, n); returns (n,) or (B, n), same
+    container kind as `Wx`."""
+    if not one_int:
+        raise NotImplementedError("`one_int=False` is not on the accelerated path")
+    is_np = isinstance(Wx, np.ndarray)
+    W = torch.as_tensor(Wx)
+    if not W.is_complex():
+        raise ValueError("`Wx` must be complex")
+    L.require_cuda()
+    W = W.to(_device_of(Wx)).contiguous()
+    is3 = W.ndim == 3
+    W3 = W if is3 else W[None]
+    B, na, n = W3.shape
+    x_len = x_len or n
+    if not isinstance(scales, (np.ndarray, torch.Tensor)) and nv is None:
+        nv = 32
+    wavelet = P.process_gmw_wavelet(wavelet, l1_norm)
+    wavelet = P.Wavelet._init_if_not_isinstance(wavelet)
+    if isinstance(scales, str):
+        sc, st, _, nv = P.process_scales(scales, x_len, wavelet, nv=nv,
+                                         get_params=True)
+    else:
+        sc, st, _, nv = P.process_scales(P._to_numpy(scales), x_len,
+                                         get_params=True)
+    sc = np.asarray(sc, np.float64).ravel()
+    if len(sc) != na:
+        raise AssertionError("%s != %s" % (len(sc), na))
+    Cpsi = P.adm_ssq(wavelet)
+    weights, mean_mult = _icwt_weights(sc, st, Cpsi, l1_norm)
+    xm = np.broadcast_to(np.asarray(x_mean, np.float64).ravel(), (B,)) \
+        if np.size(x_mean) in (1, B) else None
+    if xm is None:
+        raise ValueError("`x_mean` must be a scalar or have one value per input")
+    prec = L.F64 if W3.dtype == torch.complex128 else L.F32
+    out = torch.empty((B, n), dtype=torch.float64 if prec else torch.float32,
+                      device=W3.device)
+    wd, xmd = _dev_f64(weights, W3.device), _dev_f64(xm, W3.device)
+    with torch.cuda.device(W3.device):
+        rc = L.load().ssqb_icwt(L.ptr(W3), L.ptr(wd), L.ptr(xmd), float(mean_mult),
+                                B, na, n, prec, L.ptr(out), L.stream_ptr())
+    L.check(rc, 'icwt')
+    out = out if is3 else out[0]
+    return out.cpu().numpy() if is_np else out
+
+
+def _icwt_weights(scales, scaletype, Cpsi, l1_norm):
+    """Per-row weights and the x_mean multiplicity of the one-integral inverse
+    (_cwt.py:422-452, 479-494)."""
+    if scaletype == 'log-piecewise':
+        idx = P.logscale_transition_idx(scales)
+        w0, _ = _icwt_weights(scales[:idx], 'log', Cpsi, l1_norm)
+        w1, _ = _icwt_weights(scales[idx:], 'log', Cpsi, l1_norm)
+        return np.concatenate([w0, w1]), 2.0  # each piece adds x_mean
+    if scaletype == 'log':
+        nv = int(np.round(1 / np.diff(np.log2(scales))[0]))
+        norm = np.ones_like(scales) if l1_norm else scales**.5
+        c = (2 / Cpsi) * np.log(2 ** (1 / nv))
+    else:
+        norm = scales if l1_norm else scales**1.5
+        c = (2 / Cpsi) * np.pi / 4
+    return c / norm, 1.0
+
+
+#### squeeze on existing transforms ##########################################
+def ssqueeze(Wx, w=None, ssq_freqs=None, scales=None, Sfs=None, fs=None, t=None,
+             squeezing='sum', maprange='maximal', wavelet=None, gamma=None,
+             was_padded=True, flipud=False, dWx=None, transform='cwt'):
+    """Synchrosqueeze an existing CWT / STFT (ssqueezing.py:13-224). Returns
+    `(Tx, ssq_freqs)` with Tx as a CUDA tensor."""
+    if transform not in ('cwt', 'stft'):
+        raise ValueError("`transform` must be one of: cwt, stft "
+                         "(got %s)" % transform)
+    if w is None and (dWx is None or gamma is None):
+        raise ValueError("if `w` is None, `dWx` and `gamma` must not be.")
+    _check_ssq_args(squeezing, maprange, 'trig')
+    if transform == 'cwt' and scales is None:
+        raise ValueError("`scales` can't be None if `transform == 'cwt'`")
+    L.require_cuda()
+    dev = _device_of(Wx)
+    W = torch.as_tensor(Wx).to(dev).contiguous()
+    W3 = W if W.ndim == 3 else W[None]
+    B, na, N = W3.shape
+    if w is not None:
+        wt = torch.as_tensor(w).to(dev).contiguous()
+        if float(wt.min()) < 0:
+            raise ValueError("found negatives in `w`")
+    dt, *_ = P.process_fs_and_t(fs, t, N)
+    if transform == 'cwt':
+        sc, cwt_st, _, nv = P.process_scales(P._to_numpy(scales), N,
+                                             get_params=True)
+        if isinstance(ssq_freqs, (np.ndarray, torch.Tensor)):
+            f = P._to_numpy(ssq_freqs).astype(np.float64).ravel()
+            logscale = P.infer_scaletype(f)[0].startswith('log')
+        else:
+            st = ssq_freqs if isinstance(ssq_freqs, str) else cwt_st
+            if ((maprange == 'maximal' or isinstance(maprange, tuple)) and
+                    st == 'log-piecewise'):
+                raise ValueError("can't have `ssq_scaletype = log-piecewise` or "
+                                 "tuple with `maprange = 'maximal'`")
+            wav = P.Wavelet._init_if_not_isinstance(wavelet) if wavelet else None
+            if wav is None and maprange != 'maximal' and \
+                    not isinstance(maprange, tuple):
+                raise ValueError(f"maprange='{maprange}' requires `wavelet`")
+            f = P.compute_associated_frequencies(sc, N, wav, st, maprange,
+                                                 was_padded, dt, 'cwt')
+            logscale = st.startswith('log')
+        const = P.squeeze_weights(sc, cwt_st, nv, 'cwt')
+        sfs = None
+    else:
+        f = P._to_numpy(ssq_freqs).astype(np.float64).ravel()
+        logscale = False
+        const = P.squeeze_weights(None, None, None, 'stft', ssq_freqs=f)
+        sfs = _dev_f64(P._to_numpy(Sfs), dev) if Sfs is not None else None
+    mode, bp = P.bin_params(f, logscale)
+    cb = L.make_bins(mode, bp, na, flipud)
+    prec = L.F64 if W3.dtype == torch.complex128 else L.F32
+    Tx = torch.empty_like(W3)
+    cst = _dev_f64(const, dev)
+    with torch.cuda.device(dev):
+        if w is not None:
+            rc = L.load().ssqb_indexed_sum(L.ptr(W3), L.ptr(wt), L.ptr(cst), cb,
+                                           B, na, N, prec, L.ptr(Tx),
+                                           L.stream_ptr())
+        else:
+            dW = torch.as_tensor(dWx).to(dev).contiguous()
+            rc = L.load().ssqb_ssqueeze_fast(L.ptr(W3), L.ptr(dW), L.ptr(sfs),
+                                             L.ptr(cst), cb, float(gamma), B, na,
+                                             N, prec, L.ptr(Tx), L.stream_ptr())
+    L.check(rc, 'ssqueeze')
+    Tx = Tx if W.ndim == 3 else Tx[0]
+    if (transform == 'cwt' and not flipud) or flipud:
+        f = f[::-1]
+    return Tx, f
+
+
+def phase_cwt(Wx, dWx, difftype='trig', gamma=None):
+    """|Im(dWx / Wx)| / 2pi, inf where |Wx| < gamma (_ssq_cwt.py:420-509)."""
+    if difftype != 'trig':
+        raise ValueError("GPU computation only supports `difftype = 'trig'`")
+    W = torch.as_tensor(Wx)
+    dW = torch.as_tensor(dWx)
+    gamma = _default_gamma('float64' if W.dtype == torch.complex128 else
+                           'float32') if gamma is None else gamma
+    return _phase(W, dW, None, gamma)
+
+
+def phase_stft(Sx, dSx, Sfs, gamma=None):
+    """|Sfs - Im(dSx / Sx) / 2pi|, inf where |Sx| < gamma
+    (_ssq_stft.py:201-246)."""
+    S = torch.as_tensor(Sx)
+    gamma = _default_gamma('float64' if S.dtype == torch.complex128 else
+                           'float32') if gamma is None else gamma
+    return _phase(S, torch.as_tensor(dSx), Sfs, gamma)
+
+
+def _phase(W, dW, Sfs, gamma):
+    # an indexed_sum-free phase transform: reuse the squeeze's phase math by
+    # running the STFT/CWT phase kernel path through ssqueeze_fast is not
+    # possible (it sums); compute with the same float64 formula on the device
+    L.require_cuda()
+    dev = _device_of(W)
+    W = W.to(dev)
+    dW = dW.to(dev)
+    c, d = W.real.double(), W.imag.double()
+    a, b = dW.real.double(), dW.imag.double()
+    ph = (b * c - a * d) / ((c * c + d * d) * 6.283185307179586)
+    if Sfs is not None:
+        s = torch.as_tensor(P._to_numpy(Sfs), dtype=torch.float64, device=dev)
+        ph = s.reshape(-1, 1) - ph
+    w = ph.abs()
+    w = torch.where(W.abs() < gamma, torch.full_like(w, float('inf')), w)
+    return w.to(W.real.dtype)
+
+
+#### STFT ####################################################################
+def _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
+               derivative, dtype, want_idx=False, want_w=False, bins=None,
+               gamma=None, flipud=False):
+    N = x.shape[-1]
+    _, fs, _ = P.process_fs_and_t(fs, t, N)
+    n_fft = n_fft or min(N // hop_len, 512)
+    if win_len is None:
+        win_len = (len(window) if isinstance(window, (np.ndarray, torch.Tensor))
+                   else n_fft)
+    dtype = P._dtype_str(dtype or P.DEFAULTS['stft_dtype'])
+    win, dwin = P.get_window(window, win_len, n_fft, derivative=True)
+    if n_fft & (n_fft - 1) or n_fft < 8 or n_fft > 4096:
+        raise NotImplementedError("n_fft must be a power of two in [8, 4096] on "
+                                  "the accelerated path (got %s)" % n_fft)
+    if len(win) != n_fft:
+        raise ValueError("window length %s != n_fft %s" % (len(win), n_fft))
+    if padtype not in L.PADTYPES:
+        raise ValueError("`padtype` must be one of %s" % list(L.PADTYPES))
+    xd, is_2d = _to_device(x, dtype, False)
+    dev = xd.device
+    B = xd.shape[0]
+    _, n1, _ = P.pad_geometry(N, N + n_fft - 1)
+    nrow = n_fft // 2 + 1
+    nframes = (N - 1) // hop_len + 1
+    Sfs = np.linspace(0, .5 * fs, nrow)
+    cdt, rdt = _CDT[dtype], _RDT[dtype]
+    Sx = torch.empty((B, nrow, nframes), dtype=cdt, device=dev)
+    dSx = torch.empty_like(Sx) if derivative else None
+    w = torch.empty((B, nrow, nframes), dtype=rdt, device=dev) if want_w else None
+    idx = (torch.empty((B, nrow, nframes), dtype=torch.uint16, device=dev)
+           if want_idx else None)
+    dwin_s = dwin * fs if modulated else dwin  # _stft.py:132-135
+    wd, dwd, sfd = _dev_f64(win, dev), _dev_f64(dwin_s, dev), _dev_f64(Sfs, dev)
+    cb = None
+    if bins is not None:
+        cb = L.make_bins(bins[0], bins[1], nrow, flipud)
+    gamma = _default_gamma(dtype) if gamma is None else gamma
+    with torch.cuda.device(dev):
+        rc = L.load().ssqb_stft(L.ptr(xd), B, N, n_fft, hop_len, n1,
+                                L.PADTYPES[padtype], 1 if modulated else 0,
+                                L.ptr(wd), L.ptr(dwd), L.ptr(sfd), cb, float(gamma),
+                                _prec(dtype), L.ptr(Sx), L.ptr(dSx), L.ptr(w),
+                                L.ptr(idx), L.stream_ptr())
+    L.check(rc, 'stft')
+    return dict(Sx=Sx, dSx=dSx, w=w, idx=idx, Sfs=Sfs, dtype=dtype, dev=dev,
+                is_2d=is_2d, B=B, nrow=nrow, nframes=nframes, fs=fs, gamma=gamma)
+
+
+def stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=None,
+         padtype='reflect', modulated=True, derivative=False, dtype=None):
+    """Short-Time Fourier Transform; returns `Sx` or `(Sx, dSx)`, CUDA tensors
+    of shape (n_fft//2 + 1, n_frames) (_stft.py:13-181)."""
+    r = _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
+                   derivative, dtype)
+    Sx, dSx = _out(r['Sx'], True, r['is_2d']), _out(r['dSx'], True, r['is_2d'])
+    return (Sx, dSx) if derivative else Sx
+
+
+def ssq_stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=None,
+             modulated=True, ssq_freqs=None, padtype='reflect', squeezing='sum',
+             gamma=None, preserve_transform=None, dtype=None, astensor=True,
+             flipud=False, get_w=False, get_dWx=False):
+    """Synchrosqueezed STFT; returns `(Tx, Sx, ssq_freqs, Sfs[, w][, dSx])`
+    (_ssq_stft.py:13-136)."""
+    if x.ndim == 2 and get_w:
+        raise NotImplementedError("`get_w=True` unsupported with batched input.")
+    _check_ssq_args(squeezing, 'maximal', 'trig')
+    if isinstance(ssq_freqs, np.ndarray) and P.infer_scaletype(ssq_freqs)[0] != 'linear':
+        raise ValueError("`ssq_freqs` must be linearly distributed for `ssq_stft`")
+    N = x.shape[-1]
+    _, fs_, _ = P.process_fs_and_t(fs, t, N)
+    nfft_ = n_fft or min(N // hop_len, 512)
+    nrow = nfft_ // 2 + 1
+    Sfs_np = np.linspace(0, .5 * fs_, nrow)
+    f = Sfs_np if ssq_freqs is None else P._to_numpy(ssq_freqs).astype(np.float64).ravel()
+    mode, bp = P.bin_params(f, False)
+    r = _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
+                   get_dWx, dtype, want_idx=True, want_w=get_w, bins=(mode, bp),
+                   gamma=gamma, flipud=flipud)
+    const = P.squeeze_weights(None, None, None, 'stft', ssq_freqs=f)
+    Tx = torch.empty_like(r['Sx'])
+    cst = _dev_f64(const, r['dev'])
+    with torch.cuda.device(r['dev']):
+        rc = L.load().ssqb_squeeze(L.ptr(r['Sx']), L.ptr(r['idx']), L.ptr(cst),
+                                   r['B'], r['nrow'], r['nframes'], r['nrow'],
+                                   _prec(r['dtype']), L.ptr(Tx), L.stream_ptr())
+    L.check(rc, 'squeeze')
+    is2 = r['is_2d']
+    Sfs_out = Sfs_np.astype(r['dtype'])
+    f_out = f.astype(r['dtype']) if ssq_freqs is None else f
+    if flipud:
+        f_out = f_out[::-1]
+    if astensor:
+        Sfs_out = torch.as_tensor(Sfs_out, device=r['dev'])
+        f_out = torch.as_tensor(np.ascontiguousarray(f_out), device=r['dev'])
+    out = [_out(Tx, astensor, is2), _out(r['Sx'], astensor, is2), f_out, Sfs_out]
+    if get_w:
+        out.append(_out(r['w'], astensor, is2))
+    if get_dWx:
+        out.append(_out(r['dSx'], astensor, is2))
+    return tuple(out)

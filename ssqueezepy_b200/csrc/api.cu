@@ -1,0 +1,345 @@
+// C-ABI layer: argument checks, per-device tables, dispatch to launchers.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include "launch.h"
+#include "../../include/ssqb.h"
+
+namespace ssqb {
+
+// Twiddle tables and the status word live in module memory (no cudaMalloc).
+static __device__ double2 g_tw_lo[1 << TW_SPLIT];
+static __device__ double2 g_tw_hi[1 << (TW_LOG - TW_SPLIT)];
+static __device__ float2 g_tw4k_f[4096];
+static __device__ double2 g_tw4k_d[4096];
+static __device__ int g_status;
+
+__global__ void init_tables_kernel() {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (1 << TW_SPLIT)) {  // exp(2 pi i t / 2^22)
+    double s, c;
+    sincospi((double)t / (double)(1 << (TW_LOG - 1)), &s, &c);
+    g_tw_lo[t] = make_double2(c, s);
+  }
+  if (t < (1 << (TW_LOG - TW_SPLIT))) {  // exp(2 pi i t 2^11 / 2^22)
+    double s, c;
+    sincospi((double)t / (double)(1 << (TW_LOG - TW_SPLIT - 1)), &s, &c);
+    g_tw_hi[t] = make_double2(c, s);
+  }
+  if (t < 4096) {  // exp(2 pi i t / 4096)
+    double s, c;
+    sincospi((double)t / 2048.0, &s, &c);
+    g_tw4k_d[t] = make_double2(c, s);
+    g_tw4k_f[t] = make_float2((float)c, (float)s);
+  }
+  if (t == 0) g_status = 0;
+}
+
+static thread_local std::string t_err;
+static std::mutex g_mu;
+static bool g_init[256];
+static Tables g_tables[256];
+
+static int fail(int code, const std::string& msg) {
+  t_err = msg;
+  return code;
+}
+
+static int cuda_fail(cudaError_t e, const char* where) {
+  return fail(SSQB_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+static int get_tables(Tables* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 256) return fail(SSQB_EINVAL, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_init[dev]) {
+    Tables t;
+    void* p;
+    if ((e = cudaGetSymbolAddress(&p, g_tw_lo))) return cuda_fail(e, "symbol tw_lo");
+    t.tw_lo = (const double2*)p;
+    if ((e = cudaGetSymbolAddress(&p, g_tw_hi))) return cuda_fail(e, "symbol tw_hi");
+    t.tw_hi = (const double2*)p;
+    if ((e = cudaGetSymbolAddress(&p, g_tw4k_f))) return cuda_fail(e, "symbol tw4k_f");
+    t.tw4k_f = (const float2*)p;
+    if ((e = cudaGetSymbolAddress(&p, g_tw4k_d))) return cuda_fail(e, "symbol tw4k_d");
+    t.tw4k_d = (const double2*)p;
+    if ((e = cudaGetSymbolAddress(&p, g_status))) return cuda_fail(e, "symbol status");
+    t.status = (int*)p;
+    init_tables_kernel<<<16, 256>>>();
+    if ((e = cudaGetLastError())) return cuda_fail(e, "init tables");
+    if ((e = cudaDeviceSynchronize())) return cuda_fail(e, "init tables sync");
+    g_tables[dev] = t;
+    g_init[dev] = true;
+  }
+  *out = g_tables[dev];
+  return SSQB_OK;
+}
+
+static bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+static int ilog2i(long long n) { int m = 0; while ((1LL << m) < n) ++m; return m; }
+
+static int check_wavelet(const ssqb_wavelet* w, WavDev* out) {
+  if (!w) return fail(SSQB_EINVAL, "wavelet is NULL");
+  if (w->kind < 0 || w->kind > 2) return fail(SSQB_EINVAL, "unknown wavelet kind");
+  out->kind = w->kind;
+  out->p0 = w->p[0]; out->p1 = w->p[1]; out->p2 = w->p[2]; out->p3 = w->p[3];
+  out->wcg = (w->kind == 1) ? std::pow(w->p[2], w->p[0]) : 0.0;
+  if (w->kind != 0 && !(w->p[0] > 0 && w->p[1] > 0))
+    return fail(SSQB_EINVAL, "GMW gamma and beta must be positive");
+  return SSQB_OK;
+}
+
+static int check_bins(const ssqb_bins* b, int na, BinDev* out) {
+  if (!b) return fail(SSQB_EINVAL, "bins is NULL");
+  if (b->mode < 0 || b->mode > 2) return fail(SSQB_EINVAL, "unknown bin mode");
+  if (b->nbins < 1 || b->nbins > 65535)
+    return fail(SSQB_EINVAL, "nbins must be in [1, 65535]");
+  if (b->nbins != na) return fail(SSQB_EINVAL, "nbins must equal the number of rows");
+  out->mode = b->mode; out->idx1 = b->idx1; out->flipud = b->flipud ? 1 : 0;
+  out->nbins = b->nbins;
+  out->p0 = b->p[0]; out->p1 = b->p[1]; out->p2 = b->p[2]; out->p3 = b->p[3];
+  if (b->mode == 0 && !(b->p[1] > 0)) return fail(SSQB_EINVAL, "dvl must be > 0");
+  if (b->mode == 1 && !(b->p[2] > 0 && b->p[3] > 0))
+    return fail(SSQB_EINVAL, "dvl0, dvl1 must be > 0");
+  if (b->mode == 2 && !(b->p[1] > 0)) return fail(SSQB_EINVAL, "dv must be > 0");
+  return SSQB_OK;
+}
+
+static size_t csize(int precision) { return precision == SSQB_F64 ? 16 : 8; }
+
+static size_t xhat_bytes(int B, int Npad) { return (size_t)B * Npad * sizeof(double2); }
+
+static size_t min_z_bytes(int B, int Npad, int precision) {
+  if (!two_pass(ilog2i(Npad))) return 0;
+  const size_t a = (size_t)B * Npad * sizeof(double2);
+  const size_t c = (size_t)B * 2 * Npad * csize(precision);
+  return a > c ? a : c;
+}
+
+}  // namespace ssqb
+
+using namespace ssqb;
+
+extern "C" {
+
+int ssqb_version(void) { return 1; }
+
+const char* ssqb_last_error(void) { return t_err.c_str(); }
+
+int ssqb_device_status(void* stream, int* status_out) {
+  Tables tb;
+  int r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, tb.status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (!e) e = cudaMemsetAsync(tb.status, 0, sizeof(int), st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) return cuda_fail(e, "device status");
+  if (status_out) *status_out = h;
+  return SSQB_OK;
+}
+
+size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
+  (void)N;
+  if (B < 1 || Npad < 1 || na < 1) return 0;
+  size_t z = 0;
+  if (two_pass(ilog2i(Npad))) {
+    const size_t per_row = (size_t)B * 2 * Npad * csize(precision);
+    size_t rows = ((size_t)48 << 20) / per_row;
+    if (rows < 1) rows = 1;
+    if (rows > (size_t)na) rows = na;
+    z = rows * per_row;
+    const size_t mz = min_z_bytes(B, Npad, precision);
+    if (z < mz) z = mz;
+  }
+  return xhat_bytes(B, Npad) + z;
+}
+
+int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_bytes) {
+  if (B < 1 || na < 1 || !is_pow2(Npad)) return -1;
+  const int m = ilog2i(Npad);
+  if (!two_pass(m)) return 2;
+  const size_t xb = xhat_bytes(B, Npad);
+  if (workspace_bytes < xb) return -1;
+  const size_t zcap = (workspace_bytes - xb) / csize(precision);
+  const int S = rows_per_tile(zcap, B, 2, m, na);
+  return 2 + 2 * ((na + S - 1) / S);
+}
+
+int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
+             const double* scales, int na, const ssqb_wavelet* wavelet, double dt,
+             const ssqb_bins* bins, double gamma, int precision,
+             void* Wx, void* dWx, void* w, uint16_t* idx,
+             void* workspace, size_t workspace_bytes, void* stream) {
+  if (!x || !scales || !Wx || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
+  if (precision != SSQB_F32 && precision != SSQB_F64)
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
+    return fail(SSQB_EUNSUPPORTED, "Npad must be a power of two in [8, 2^22]");
+  if (Npad < N || n1 < 0 || n1 + N > Npad) return fail(SSQB_EINVAL, "bad padding geometry");
+  if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
+  if (!(dt > 0)) return fail(SSQB_EINVAL, "dt must be > 0");
+  if (B > 65535 || na > 65535) return fail(SSQB_EINVAL, "B and na must be <= 65535");
+  WavDev wd;
+  int r = check_wavelet(wavelet, &wd);
+  if (r) return r;
+  BinDev bd{};
+  if (idx) {
+    r = check_bins(bins, na, &bd);
+    if (r) return r;
+  }
+  const size_t need = xhat_bytes(B, Npad) + min_z_bytes(B, Npad, precision);
+  if (workspace_bytes < need)
+    return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                     " bytes");
+  Tables tb;
+  r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* xh = (double2*)workspace;
+  unsigned char* zb = (unsigned char*)workspace + xhat_bytes(B, Npad);
+  const size_t zbytes = workspace_bytes - xhat_bytes(B, Npad);
+  int e;
+  if (precision == SSQB_F32)
+    e = run_xhat_f32((const float*)x, B, N, Npad, n1, padtype, xh, (double2*)zb,
+                     zbytes / sizeof(double2), tb, st);
+  else
+    e = run_xhat_f64((const double*)x, B, N, Npad, n1, padtype, xh, (double2*)zb,
+                     zbytes / sizeof(double2), tb, st);
+  if (e) return cuda_fail((cudaError_t)e, "x_hat launch");
+  const int m = ilog2i(Npad);
+  const double h = (2 * M_PI) / Npad;
+  const int oN = rpadded ? Npad : N, on1 = rpadded ? 0 : n1;
+  if (precision == SSQB_F32) {
+    CwtOp<float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,
+                     (float)(1.0 / Npad), gamma, (float2*)Wx, (float2*)dWx, (float*)w,
+                     idx, tb.status};
+    e = run_cwt_f32(op, B, m, (float2*)zb, zbytes / sizeof(float2), tb, st);
+  } else {
+    CwtOp<double2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt, 1.0 / Npad,
+                      gamma, (double2*)Wx, (double2*)dWx, (double*)w, idx, tb.status};
+    e = run_cwt_f64(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st);
+  }
+  if (e) return cuda_fail((cudaError_t)e, "cwt launch");
+  return SSQB_OK;
+}
+
+static int squeeze_common(const void* Wx, int kind, const void* src, const double* sfs,
+                          const double* cst, const ssqb_bins* bins, double gamma, int B,
+                          int na, int N, int nbins, int precision, void* Tx, void* stream) {
+  if (!Wx || !src || !cst || !Tx) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
+  if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
+  if (precision != SSQB_F32 && precision != SSQB_F64)
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  if (nbins < 1 || nbins > 65535) return fail(SSQB_EINVAL, "nbins must be in [1, 65535]");
+  BinDev bd{};
+  if (kind != 0) {
+    int r = check_bins(bins, nbins, &bd);
+    if (r) return r;
+  }
+  const size_t smem = (size_t)nbins * 32 * csize(precision) +
+                      (size_t)na * (precision == SSQB_F64 ? 8 : 4);
+  if (smem > 227 * 1024)
+    return fail(SSQB_EUNSUPPORTED, "too many bins for the shared-memory squeeze");
+  Tables tb;
+  int r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  int e;
+  if (precision == SSQB_F32)
+    e = run_squeeze_f32((const float2*)Wx, kind, src, sfs, bd, gamma, cst, B, na, N, nbins,
+                        (float2*)Tx, tb.status, st);
+  else
+    e = run_squeeze_f64((const double2*)Wx, kind, src, sfs, bd, gamma, cst, B, na, N, nbins,
+                        (double2*)Tx, tb.status, st);
+  if (e) return cuda_fail((cudaError_t)e, "squeeze launch");
+  return SSQB_OK;
+}
+
+int ssqb_squeeze(const void* Wx, const uint16_t* idx, const double* row_weights, int B,
+                 int na, int N, int nbins, int precision, void* Tx, void* stream) {
+  return squeeze_common(Wx, 0, idx, nullptr, row_weights, nullptr, 0.0, B, na, N, nbins,
+                        precision, Tx, stream);
+}
+
+int ssqb_ssqueeze_fast(const void* Wx, const void* dWx, const double* Sfs,
+                       const double* row_weights, const ssqb_bins* bins, double gamma,
+                       int B, int na, int N, int precision, void* Tx, void* stream) {
+  return squeeze_common(Wx, 1, dWx, Sfs, row_weights, bins, gamma, B, na, N,
+                        bins ? bins->nbins : 0, precision, Tx, stream);
+}
+
+int ssqb_indexed_sum(const void* Wx, const void* w, const double* row_weights,
+                     const ssqb_bins* bins, int B, int na, int N, int precision, void* Tx,
+                     void* stream) {
+  return squeeze_common(Wx, 2, w, nullptr, row_weights, bins, 0.0, B, na, N,
+                        bins ? bins->nbins : 0, precision, Tx, stream);
+}
+
+int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padtype,
+              int modulated, const double* window, const double* diff_window,
+              const double* Sfs, const ssqb_bins* bins, double gamma, int precision,
+              void* Sx, void* dSx, void* w, uint16_t* idx, void* stream) {
+  if (!x || !window || !diff_window || !Sfs || !Sx)
+    return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || hop < 1) return fail(SSQB_EINVAL, "B, N and hop must be >= 1");
+  if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
+  if (!is_pow2(n_fft) || n_fft < 8 || n_fft > 4096)
+    return fail(SSQB_EUNSUPPORTED, "n_fft must be a power of two in [8, 4096]");
+  if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
+  if (precision != SSQB_F32 && precision != SSQB_F64)
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  const int nrow = n_fft / 2 + 1;
+  BinDev bd{};
+  if (idx) {
+    int r = check_bins(bins, nrow, &bd);
+    if (r) return r;
+  }
+  Tables tb;
+  int r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nframes = (N - 1) / hop + 1;
+  const int s20 = (n_fft + 1) / 2;
+  const int s21 = (n_fft % 2 == 1) ? s20 - 1 : s20;
+  const int m = ilog2i(n_fft);
+  int e;
+  if (precision == SSQB_F32) {
+    StftOp<float, float2> op{(const float*)x, window, diff_window, Sfs, bd, N, n_fft, hop,
+                             n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
+                             (float2*)Sx, (float2*)dSx, (float*)w, idx, tb.status};
+    e = run_stft_f32(op, B, m, tb, st);
+  } else {
+    StftOp<double, double2> op{(const double*)x, window, diff_window, Sfs, bd, N, n_fft,
+                               hop, n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
+                               (double2*)Sx, (double2*)dSx, (double*)w, idx, tb.status};
+    e = run_stft_f64(op, B, m, tb, st);
+  }
+  if (e) return cuda_fail((cudaError_t)e, "stft launch");
+  return SSQB_OK;
+}
+
+int ssqb_icwt(const void* Wx, const double* row_weights, const double* x_mean,
+              double mean_weight, int B, int na, int N, int precision, void* x,
+              void* stream) {
+  if (!Wx || !row_weights || !x) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
+  if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
+  if (precision != SSQB_F32 && precision != SSQB_F64)
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  int e = run_icwt(Wx, row_weights, x_mean, mean_weight, B, na, N, precision, x,
+                   (cudaStream_t)stream);
+  if (e) return cuda_fail((cudaError_t)e, "icwt launch");
+  return SSQB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+// Squeeze kernel instantiations and launchers.
+#include "launch.h"
+#include "squeeze.cuh"
+
+namespace ssqb {
+
+template <typename C, class Src>
+static int launch_sq(const C* Wx, const Src& src, const double* cst, int B, int na, int N,
+                     int nbins, C* Tx, int* status, cudaStream_t st) {
+  typedef typename RealOf<C>::type T;
+  const size_t smem = (size_t)nbins * 32 * sizeof(C) + (size_t)na * sizeof(T);
+  auto k = squeeze_kernel<C, Src>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  dim3 grid((N + 31) / 32, B);
+  k<<<grid, 32, smem, st>>>(Wx, src, cst, na, N, nbins, Tx, status);
+  return cudaGetLastError();
+}
+
+template <typename C>
+static int run_sq(const C* Wx, int src_kind, const void* src, const double* sfs,
+                  const BinDev& bins, double gamma, const double* cst, int B, int na, int N,
+                  int nbins, C* Tx, int* status, cudaStream_t st) {
+  typedef typename RealOf<C>::type T;
+  switch (src_kind) {
+    case 0: {
+      IdxSrc<C> s{(const uint16_t*)src};
+      return launch_sq(Wx, s, cst, B, na, N, nbins, Tx, status, st);
+    }
+    case 1: {
+      PhaseSrc<C> s{(const C*)src, sfs, bins, gamma, status};
+      return launch_sq(Wx, s, cst, B, na, N, nbins, Tx, status, st);
+    }
+    case 2: {
+      WSrc<C> s{(const T*)src, bins, status};
+      return launch_sq(Wx, s, cst, B, na, N, nbins, Tx, status, st);
+    }
+    default:
+      return (int)cudaErrorInvalidValue;
+  }
+}
+
+int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, const double* sfs,
+                    const BinDev& bins, double gamma, const double* cst, int B, int na,
+                    int N, int nbins, float2* Tx, int* status, cudaStream_t st) {
+  return run_sq<float2>(Wx, src_kind, src, sfs, bins, gamma, cst, B, na, N, nbins, Tx,
+                        status, st);
+}
+
+int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, const double* sfs,
+                    const BinDev& bins, double gamma, const double* cst, int B, int na,
+                    int N, int nbins, double2* Tx, int* status, cudaStream_t st) {
+  return run_sq<double2>(Wx, src_kind, src, sfs, bins, gamma, cst, B, na, N, nbins, Tx,
+                         status, st);
+}
+
+}  // namespace ssqb
+
+namespace ssqb {
+
+// x[b, j] = sum_i Re Wx[b, i, j] * w_i + x_mean[b] * mw; one thread per
+// column, rows in ascending order (float64 accumulation).
+template <typename C>
+__global__ void icwt_kernel(const C* __restrict__ Wx, const double* __restrict__ w,
+                            const double* __restrict__ x_mean, double mw, int na, int N,
+                            typename RealOf<C>::type* __restrict__ x) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (j >= N) return;
+  const C* p = Wx + (size_t)b * na * N + j;
+  double acc = 0.0;
+  int i = 0;
+  for (; i + 4 <= na; i += 4) {
+    const double r0 = (double)p[(size_t)(i + 0) * N].x, r1 = (double)p[(size_t)(i + 1) * N].x;
+    const double r2 = (double)p[(size_t)(i + 2) * N].x, r3 = (double)p[(size_t)(i + 3) * N].x;
+    acc += r0 * w[i];
+    acc += r1 * w[i + 1];
+    acc += r2 * w[i + 2];
+    acc += r3 * w[i + 3];
+  }
+  for (; i < na; ++i) acc += (double)p[(size_t)i * N].x * w[i];
+  if (x_mean) acc += x_mean[b] * mw;
+  x[(size_t)b * N + j] = (typename RealOf<C>::type)acc;
+}
+
+int run_icwt(const void* Wx, const double* w, const double* x_mean, double mean_weight,
+             int B, int na, int N, int precision, void* x, cudaStream_t st) {
+  dim3 grid((N + 255) / 256, B);
+  if (precision == 0)
+    icwt_kernel<float2><<<grid, 256, 0, st>>>((const float2*)Wx, w, x_mean, mean_weight, na,
+                                              N, (float*)x);
+  else
+    icwt_kernel<double2><<<grid, 256, 0, st>>>((const double2*)Wx, w, x_mean, mean_weight,
+                                               na, N, (double*)x);
+  return cudaGetLastError();
+}
+
+}  // namespace ssqb

@@ -1,0 +1,50 @@
+// Host-side launchers shared between the kernel translation units and the
+// C-ABI layer. Each returns 0 or a cudaError_t value.
+#pragma once
+#include <cuda_runtime.h>
+#include "ssqb_ops.cuh"
+
+namespace ssqb {
+
+// row tile of the two-pass transform: rows whose intermediate fits in zcap
+// complex elements (at least one row)
+inline int rows_per_tile(size_t zcap_elems, int B, int narr, int log2L, int nrows) {
+  const size_t per = (size_t)B * narr * ((size_t)1 << log2L);
+  size_t s = per ? zcap_elems / per : 0;
+  if (s < 1) s = 1;
+  if (s > (size_t)nrows) s = nrows;
+  if (s > 65535) s = 65535;
+  return (int)s;
+}
+
+// single-pass when L <= 4096; else two passes with log2(L2) = m/2
+constexpr int kTile = 4096;
+inline bool two_pass(int log2L) { return log2L > 12; }
+
+int run_xhat_f32(const float* x, int B, int N, int Npad, int n1, int padtype,
+                 double2* xh, double2* Z, size_t zcap, const Tables& tb,
+                 cudaStream_t st);
+int run_xhat_f64(const double* x, int B, int N, int Npad, int n1, int padtype,
+                 double2* xh, double2* Z, size_t zcap, const Tables& tb,
+                 cudaStream_t st);
+int run_cwt_f32(const CwtOp<float2>& op, int B, int log2L, float2* Z, size_t zcap,
+                const Tables& tb, cudaStream_t st);
+int run_cwt_f64(const CwtOp<double2>& op, int B, int log2L, double2* Z, size_t zcap,
+                const Tables& tb, cudaStream_t st);
+int run_stft_f32(const StftOp<float, float2>& op, int B, int log2L,
+                 const Tables& tb, cudaStream_t st);
+int run_stft_f64(const StftOp<double, double2>& op, int B, int log2L,
+                 const Tables& tb, cudaStream_t st);
+
+// squeeze; src_kind 0 = uint16 index, 1 = phase from dWx (cwt or stft), 2 = w
+int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, const double* sfs,
+                    const BinDev& bins, double gamma, const double* cst, int B, int na,
+                    int N, int nbins, float2* Tx, int* status, cudaStream_t st);
+int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, const double* sfs,
+                    const BinDev& bins, double gamma, const double* cst, int B, int na,
+                    int N, int nbins, double2* Tx, int* status, cudaStream_t st);
+
+int run_icwt(const void* Wx, const double* w, const double* x_mean, double mean_weight,
+             int B, int na, int N, int precision, void* x, cudaStream_t st);
+
+}  // namespace ssqb

@@ -1,0 +1,251 @@
+// Prologue/epilogue operators for the tile FFT kernels: padded-signal FFT
+// (x_hat), fused CWT (wavelet x x_hat -> Wx, dWx -> phase transform -> bin),
+// fused STFT (framing + windows -> Sx, dSx -> phase transform -> bin).
+#pragma once
+#include "tile_kernels.cuh"
+
+namespace ssqb {
+
+// ---- parameters passed by value ------------------------------------------
+struct WavDev {
+  int kind;          // 0 Morlet, 1 GMW L1 (bandpass), 2 GMW L2 (energy)
+  double p0, p1, p2, p3;  // Morlet: mu, ks, C1; GMW: gamma, beta, wc, wcl | l2norm
+  double wcg;        // GMW: wc^gamma
+};
+
+struct BinDev {
+  int mode;          // 0 log, 1 log-piecewise, 2 linear
+  int idx1;
+  int flipud;
+  int nbins;         // omax + 1
+  double p0, p1, p2, p3;  // log: vlmin, dvl | piecewise: vlmin0, vlmin1, dvl0, dvl1 | lin: vmin, dv
+};
+
+constexpr uint16_t kNoBin = 0xFFFF;
+constexpr double kTwoPi = 6.283185307179586;  // the literal of algos.py:867
+
+// ---- padding index map (utils/common.py:54-158) -------------------------
+// q: position relative to x[0]; returns the source index, or -1 for a zero.
+enum PadType { PAD_ZERO = 0, PAD_REFLECT = 1, PAD_SYMMETRIC = 2, PAD_REPLICATE = 3,
+               PAD_WRAP = 4, PAD_NONE = 5 };
+
+__device__ __forceinline__ int pad_src(long long q, int N, int padtype) {
+  if (q >= 0 && q < N) return (int)q;
+  switch (padtype) {
+    case PAD_REFLECT: {  // numpy 'reflect': period 2(N-1), no edge repeat
+      if (N == 1) return 0;
+      long long P = 2LL * (N - 1);
+      long long r = q % P;
+      if (r < 0) r += P;
+      return (int)(r >= N ? P - r : r);
+    }
+    case PAD_SYMMETRIC: {  // edge repeated: period 2N
+      long long P = 2LL * N;
+      long long r = q % P;
+      if (r < 0) r += P;
+      return (int)(r >= N ? P - 1 - r : r);
+    }
+    case PAD_REPLICATE:
+      return q < 0 ? 0 : N - 1;
+    case PAD_WRAP: {
+      long long r = q % N;
+      if (r < 0) r += N;
+      return (int)r;
+    }
+    default:
+      return -1;
+  }
+}
+
+// ---- wavelets, float64 (wavelets.py:521-527, _gmw.py:203-210, 246-251) --
+__device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
+  if (w.kind == 0) {
+    const double d = x - w.p0;
+    const double a = -0.5 * (d * d);
+    const double c = -0.5 * (x * x);
+    const double ea = a > -708.0 ? exp(a) : 0.0;
+    const double ec = c > -708.0 ? exp(c) : 0.0;
+    return w.p2 * (ea - w.p1 * ec);
+  }
+  if (x <= 0.0) return 0.0;
+  const double lw = log(x);
+  const double xg = (w.p0 == 3.0) ? x * x * x : exp(w.p0 * lw);
+  if (w.kind == 1) {
+    const double e = -w.p1 * w.p3 + w.wcg + w.p1 * lw - xg;
+    return e > -708.0 ? 2.0 * exp(e) : 0.0;
+  }
+  // L2: norm * x^beta * exp(-x^gamma)
+  const double e = w.p1 * lw - xg;
+  return e > -708.0 ? w.p3 * exp(e) : 0.0;
+}
+
+// ---- frequency bin (algos.py:859-953; round = half-to-even, as numba) ----
+__device__ __forceinline__ int bin_of(const BinDev& bp, double w) {
+  const double omax = (double)(bp.nbins - 1);
+  double k;
+  if (bp.mode == 2) {
+    k = fmin(rint(fmax((w - bp.p0) / bp.p1, 0.0)), omax);
+  } else {
+    const double wl = log2(w);
+    if (bp.mode == 0) {
+      k = fmin(rint(fmax((wl - bp.p0) / bp.p1, 0.0)), omax);
+    } else if (wl > bp.p1) {
+      k = fmin(rint((wl - bp.p1) / bp.p3) + (double)bp.idx1, omax);
+    } else {
+      k = fmax(rint((wl - bp.p0) / bp.p2), 0.0);
+    }
+  }
+  int ki = (int)k;
+  if (bp.flipud) ki = bp.nbins - 1 - ki;
+  return ki;
+}
+
+// Phase transform and bin of one (Wx, dWx) pair, float64 from the stored
+// values (algos.py:864-876): w = |Im(dWx conj Wx)| / (|Wx|^2 2pi), Sfs shift
+// for the STFT (algos.py:963-964). Returns kNoBin where |Wx| <= gamma.
+template <typename C>
+__device__ __forceinline__ uint16_t phase_bin(C Wv, C dWv, double sfs, bool stft,
+                                              const BinDev& bp, double gamma,
+                                              int* status, double* w_out) {
+  const double c = Wv.x, d = Wv.y, a = dWv.x, b = dWv.y;
+  const double m2 = c * c + d * d;
+  const double mag = sqrt(m2);
+  const double ph = (b * c - a * d) / (m2 * kTwoPi);
+  const double w = stft ? fabs(sfs - ph) : fabs(ph);
+  if (w_out) *w_out = (mag < gamma) ? __longlong_as_double(0x7ff0000000000000ULL) : w;
+  if (!(mag > gamma)) return kNoBin;
+  const int k = bin_of(bp, w);
+  if (k < 0 || k >= bp.nbins || k >= (int)kNoBin) {
+    set_status(status, DEV_BAD_BIN);
+    return kNoBin;
+  }
+  return (uint16_t)k;
+}
+
+template <typename C> __device__ __forceinline__ void put_w(C* p, double v);
+template <> __device__ __forceinline__ void put_w<float2>(float2* p, double v) {
+  reinterpret_cast<float*>(p)[0] = (float)v;
+}
+template <> __device__ __forceinline__ void put_w<double2>(double2* p, double v) {
+  reinterpret_cast<double*>(p)[0] = v;
+}
+
+// ---- x_hat: FFT of the padded signal, float64 ------------------------------
+template <typename TX>
+struct XhatOp {
+  static constexpr int NARR = 1;
+  static constexpr bool kStoreRowFast = false;
+  const TX* x;       // (B, N)
+  double2* xh;       // (B, Npad)
+  int N, Npad, n1, padtype;
+  __device__ int rows() const { return 1; }
+  __device__ void load(int b, int, int k, double2 (&v)[1]) const {
+    const int s = pad_src((long long)k - n1, N, padtype);
+    v[0] = make_double2(s >= 0 ? (double)x[(size_t)b * N + s] : 0.0, 0.0);
+  }
+  __device__ void store(int b, int, int n, double2* const (&seq)[1], int pos, int) const {
+    xh[(size_t)b * Npad + n] = seq[0][spad(pos)];
+  }
+};
+
+// ---- fused CWT ---------------------------------------------------------------
+template <typename C>
+struct CwtOp {
+  typedef typename RealOf<C>::type T;
+  static constexpr int NARR = 2;
+  static constexpr bool kStoreRowFast = false;
+  const double2* xh;      // (B, Npad) float64
+  const double* scales;   // (na)
+  WavDev wav;
+  BinDev bins;
+  int na, N, Npad, n1;    // N, n1: output width and the padded index of its first column
+  double h;               // 2*pi / Npad
+  double inv_dt;
+  T inv_npad;
+  double gamma;
+  C* Wx;                  // (B, na, N)
+  C* dWx;                 // optional
+  T* w;                   // optional phase transform
+  uint16_t* idx;          // optional bin index
+  int* status;
+  __device__ int rows() const { return na; }
+  __device__ void load(int b, int row, int k, C (&v)[2]) const {
+    const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
+    const double xi = (double)kk * h;
+    double ps = psih_fp64(wav, scales[row] * xi);
+    if (k == (Npad >> 1)) ps *= 0.5;  // Nyquist bin halved (wavelets.py:86-95)
+    const double2 xv = __ldg(xh + (size_t)b * Npad + k);
+    const double2 y = make_double2(ps * xv.x, ps * xv.y);
+    const double c = xi * inv_dt;
+    v[0] = to_c<C>(y);
+    v[1] = to_c<C>(make_double2(-y.y * c, y.x * c));
+  }
+  __device__ void store(int b, int row, int n, C* const (&seq)[2], int pos, int) const {
+    const int j = n - n1;
+    if (j < 0 || j >= N) return;
+    C Wv = seq[0][spad(pos)], dWv = seq[1][spad(pos)];
+    Wv.x *= inv_npad; Wv.y *= inv_npad;
+    dWv.x *= inv_npad; dWv.y *= inv_npad;
+    const size_t o = ((size_t)b * na + row) * N + j;
+    if (Wx) Wx[o] = Wv;
+    if (dWx) dWx[o] = dWv;
+    if (idx || w) {
+      double wv;
+      const uint16_t k = phase_bin(Wv, dWv, 0.0, false, bins, gamma, status,
+                                   w ? &wv : nullptr);
+      if (idx) idx[o] = k;
+      if (w) w[o] = (T)wv;
+    }
+  }
+};
+
+// ---- fused STFT (modulated framing, stft_utils.py:69-98; _stft.py:127-147)
+template <typename TX, typename C>
+struct StftOp {
+  typedef typename RealOf<C>::type T;
+  static constexpr int NARR = 1;
+  static constexpr bool kStoreRowFast = true;
+  const TX* x;             // (B, N)
+  const double* win;       // (n_fft)
+  const double* dwin;      // (n_fft), already times fs
+  const double* sfs;       // (n_fft/2 + 1)
+  BinDev bins;
+  int N, L, hop, n1, padtype, s21, modulated, nframes;
+  double gamma;
+  C* Sx;                   // (B, L/2+1, nframes)
+  C* dSx;
+  T* w;
+  uint16_t* idx;
+  int* status;
+  __device__ int rows() const { return nframes; }
+  __device__ void load(int b, int t, int m, C (&v)[1]) const {
+    const int q = modulated ? ((m + s21) & (L - 1)) : m;
+    const long long p = (long long)t * hop + q;  // position in the padded signal
+    const int s = pad_src(p - n1, N, padtype);
+    const double xv = s >= 0 ? (double)x[(size_t)b * N + s] : 0.0;
+    v[0] = to_c<C>(make_double2(xv * __ldg(win + q), xv * __ldg(dwin + q)));
+  }
+  __device__ void store(int b, int t, int n, C* const (&seq)[1], int, int rowbase) const {
+    const int nrow = (L >> 1) + 1;
+    if (n >= nrow) return;
+    const C zk = seq[0][spad(rowbase + n)];
+    const C zm = seq[0][spad(rowbase + ((L - n) & (L - 1)))];
+    const T hf = (T)0.5;
+    // z = a + i*b with real a (window) and b (diff window):
+    // A_k = (Z_k + conj Z_{L-k}) / 2,  B_k = (Z_k - conj Z_{L-k}) / (2i)
+    const C S = mk(hf * (zk.x + zm.x), hf * (zk.y - zm.y));
+    const C dS = mk(hf * (zk.y + zm.y), -hf * (zk.x - zm.x));
+    const size_t o = ((size_t)b * nrow + n) * nframes + t;
+    if (Sx) Sx[o] = S;
+    if (dSx) dSx[o] = dS;
+    if (idx || w) {
+      double wv;
+      const uint16_t k = phase_bin(S, dS, __ldg(sfs + n), true, bins, gamma, status,
+                                   w ? &wv : nullptr);
+      if (idx) idx[o] = k;
+      if (w) w[o] = (T)wv;
+    }
+  }
+};
+
+}  // namespace ssqb

@@ -1,0 +1,220 @@
+# -*- coding: utf-8 -*-
+"""Parity of the CUDA path (through the C ABI) with ssqueezepy's float64
+outputs (golden fixtures) and with the float64 oracle.
+
+Tolerances: float64 transforms must agree to 1e-10 relative L2 (Wx, Tx);
+float32 transforms follow the required bars, relative L2 <= 1e-5 on Wx and
+<= 1e-4 on Tx, against the float64 results."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssq_oracle as O
+from ssqueezepy_b200 import _params as P
+from tests._cases import (WAVS, CWT_CASES, STFT_CASES, oracle_kind, rel_l2,
+                          chirp_signal)
+
+pytestmark = pytest.mark.gpu
+
+WX_TOL_F32, TX_TOL_F32 = 1e-5, 1e-4
+TOL_F64 = 1e-10
+
+
+@pytest.fixture(scope='module')
+def sb():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    import ssqueezepy_b200 as m
+    m._lib.load()
+    return m
+
+
+@pytest.fixture(autouse=True)
+def _status_clean(sb):
+    yield
+    assert sb._lib.device_status() == 0
+
+
+def _np(t):
+    return t.detach().cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
+def _case_args(g, name, dtype):
+    wk, st, sqf, mr, pad, flip = [str(v) for v in g[f'{name}/cfg']]
+    nm, opts = WAVS[wk]
+    wav = P.Wavelet((nm, dict(opts, dtype=dtype)))
+    return dict(wavelet=wav, scales=st, nv=32,
+                ssq_freqs=None if sqf == 'None' else sqf, maprange=mr,
+                padtype=pad, flipud=(flip == 'True'))
+
+
+@pytest.mark.parametrize('name', CWT_CASES)
+def test_ssq_cwt_f64_matches_reference(sb, golden_transforms, name):
+    g = golden_transforms
+    kw = _case_args(g, name, 'float64')
+    Tx, Wx, f, s = sb.ssq_cwt(g[f'{name}/x'], **kw)
+    assert rel_l2(_np(Wx), g[f'{name}/Wx']) < TOL_F64
+    assert rel_l2(_np(Tx), g[f'{name}/Tx']) < TOL_F64
+    assert np.array_equal(np.asarray(f), g[f'{name}/ssq_freqs'])
+    assert np.array_equal(_np(s), g[f'{name}/scales'])
+    assert _np(Tx).dtype == np.complex128 and np.asarray(f).dtype == np.float64
+
+
+@pytest.mark.parametrize('name', CWT_CASES)
+def test_ssq_cwt_f32_tolerance(sb, golden_transforms, name):
+    g = golden_transforms
+    kw = _case_args(g, name, 'float32')
+    Tx, Wx, f, s = sb.ssq_cwt(g[f'{name}/x'], **kw)
+    assert _np(Tx).dtype == np.complex64 and _np(s).dtype == np.float32
+    assert rel_l2(_np(Wx), g[f'{name}/Wx']) < WX_TOL_F32
+    assert rel_l2(_np(Tx), g[f'{name}/Tx']) < TX_TOL_F32
+
+
+def test_get_w_and_dwx(sb, golden_transforms):
+    g = golden_transforms
+    kw = _case_args(g, 'c0', 'float64')
+    Tx, Wx, f, s, w, dWx = sb.ssq_cwt(g['c0/x'], get_w=True, get_dWx=True, **kw)
+    wr = g['c0/w']
+    fin = np.isfinite(wr)
+    assert np.array_equal(fin, np.isfinite(_np(w)))
+    assert np.allclose(_np(w)[fin], wr[fin], rtol=1e-9, atol=0)
+    c = O.cwt(g['c0/x'], 'morlet', (6.,), g['c0/scales'])
+    assert rel_l2(_np(dWx), c[1]) < TOL_F64
+
+
+def test_batched_equals_reference(sb, golden_transforms):
+    g = golden_transforms
+    w = P.Wavelet(('morlet', {'mu': 6., 'dtype': 'float64'}))
+    Tx, Wx, f, s = sb.ssq_cwt(g['b0/x'], w, scales='log-piecewise', nv=32,
+                              ssq_freqs='log')
+    assert _np(Tx).shape == g['b0/Tx'].shape
+    assert rel_l2(_np(Wx), g['b0/Wx']) < TOL_F64
+    assert rel_l2(_np(Tx), g['b0/Tx']) < TOL_F64
+    # batched == looped, as the reference's test_ssq_cwt_batched checks
+    for i in range(len(g['b0/x'])):
+        Ti, *_ = sb.ssq_cwt(g['b0/x'][i], w, scales='log-piecewise', nv=32,
+                            ssq_freqs='log')
+        assert np.array_equal(_np(Ti), _np(Tx)[i])
+
+
+@pytest.mark.parametrize('name', CWT_CASES)
+def test_icwt_matches_reference(sb, golden_transforms, name):
+    g = golden_transforms
+    kw = _case_args(g, name, 'float64')
+    x = sb.icwt(g[f'{name}/Wx'], kw['wavelet'], scales=g[f'{name}/scales'],
+                x_mean=g[f'{name}/x'].mean())
+    assert np.allclose(x, g[f'{name}/icwt'], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize('name', STFT_CASES)
+@pytest.mark.parametrize('dtype', ['float64', 'float32'])
+def test_ssq_stft_matches_reference(sb, golden_transforms, name, dtype):
+    g = golden_transforms
+    win, n_fft, win_len, hop = [str(v) for v in g[f'{name}/cfg']]
+    Tx, Sx, f, Sfs = sb.ssq_stft(g[f'{name}/x'], window=None if win == 'None' else win,
+                                 n_fft=int(n_fft), win_len=int(win_len),
+                                 hop_len=int(hop), dtype=dtype)
+    tol_s, tol_t = (TOL_F64, TOL_F64) if dtype == 'float64' else (WX_TOL_F32, TX_TOL_F32)
+    assert rel_l2(_np(Sx), g[f'{name}/Sx']) < tol_s
+    assert rel_l2(_np(Tx), g[f'{name}/Tx']) < tol_t
+    assert np.allclose(_np(Sfs), g[f'{name}/Sfs'])
+
+
+def test_stft_derivative_and_w(sb, golden_transforms):
+    g = golden_transforms
+    window, dwin = P.get_window('hann', 128, 128, derivative=True)
+    Sx, dSx = sb.stft(g['s0/x'], 'hann', n_fft=128, derivative=True, dtype='float64')
+    S_o, dS_o = O.stft(g['s0/x'], window, dwin, 128)
+    assert rel_l2(_np(Sx), S_o) < TOL_F64
+    assert rel_l2(_np(dSx), dS_o) < TOL_F64
+    *_, w = sb.ssq_stft(g['s0/x'], 'hann', n_fft=128, dtype='float64', get_w=True)
+    wr = g['s0/w']
+    fin = np.isfinite(wr)
+    assert np.allclose(_np(w)[fin], wr[fin], rtol=1e-9, atol=1e-12)
+
+
+def test_cwt_api_and_padtypes(sb):
+    x = chirp_signal(1000, seed=3)
+    scales = P.process_scales('log-piecewise', 1000,
+                              P.Wavelet(('morlet', {'mu': 6.})), nv=32)
+    for pad in ('reflect', 'zero', 'symmetric', 'replicate', 'wrap'):
+        Wx, s, dWx = sb.cwt(x, ('morlet', {'mu': 6., 'dtype': 'float64'}),
+                            scales='log-piecewise', padtype=pad, derivative=True)
+        Wo, dWo = O.cwt(x, 'morlet', (6.,), scales, padtype=pad)
+        assert rel_l2(_np(Wx), Wo) < TOL_F64, pad
+        assert rel_l2(_np(dWx), dWo) < TOL_F64, pad
+    # rpadded keeps all padded columns
+    Wx, _ = sb.cwt(x, ('morlet', {'mu': 6., 'dtype': 'float64'}), rpadded=True)
+    assert _np(Wx).shape[-1] == P.p2up(1000)[0]
+
+
+def test_ssqueeze_api_paths_agree(sb, golden_transforms):
+    """ssqueeze from (Wx, dWx) and from w give the fused path's Tx."""
+    g = golden_transforms
+    kw = _case_args(g, 'c0', 'float64')
+    Tx, Wx, f, s, w, dWx = sb.ssq_cwt(g['c0/x'], get_w=True, get_dWx=True, **kw)
+    T1, f1 = sb.ssqueeze(Wx, None, ssq_freqs=f[::-1].copy(), scales=s,
+                         dWx=dWx, gamma=10 * P.EPS64, flipud=True)
+    T2, _ = sb.ssqueeze(Wx, w, ssq_freqs=f[::-1].copy(), scales=s, flipud=True)
+    assert np.array_equal(_np(T1), _np(Tx))
+    assert np.array_equal(_np(T2), _np(Tx))
+
+
+def _full_size(sb, N, wk, sqf, dtype):
+    x = chirp_signal(N, seed=0)
+    nm, opts = WAVS[wk]
+    wav = P.Wavelet((nm, dict(opts, dtype=dtype)))
+    Tx, Wx, f, s = sb.ssq_cwt(x, wav, scales='log-piecewise', nv=32,
+                              ssq_freqs=sqf)
+    return x, _np(Tx), _np(Wx), np.asarray(f), _np(s).astype(np.float64)
+
+
+@pytest.mark.parametrize('N, wk, sqf', [(10000, 'morlet6', 'log'),
+                                        (160000, 'gmw3_60', None)])
+def test_full_size_f32_vs_oracle(sb, golden_digests, N, wk, sqf):
+    """The N=10,000 Morlet and N=160,000 GMW single-signal workloads in
+    float32 against the float64 oracle (pinned by the golden digests)."""
+    x, Tx, Wx, f, s = _full_size(sb, N, wk, sqf, 'float32')
+    key = 'd10k' if N == 10000 else 'd160k'
+    assert np.array_equal(f, golden_digests[f'{key}/ssq_freqs'])
+    _, st, _, nv = P.process_scales(s, N, get_params=True)
+    const = P.squeeze_weights(s, st, nv, 'cwt')
+    To, Wo, _ = O.ssq_cwt(x, *oracle_kind(wk), s, f[::-1], const)
+    assert np.allclose(np.linalg.norm(Wo, axis=1), golden_digests[f'{key}/Wx_rownorm'],
+                       rtol=1e-9)
+    ew, et = rel_l2(Wx, Wo), rel_l2(Tx, To)
+    print(f'\n{key} float32: Wx rel-L2 {ew:.3e}  Tx rel-L2 {et:.3e}')
+    assert ew < WX_TOL_F32
+    assert et < TX_TOL_F32
+
+
+def test_deterministic(sb):
+    x = chirp_signal(20000, seed=7)
+    a = _np(sb.ssq_cwt(x, ('gmw', {}))[0])
+    b = _np(sb.ssq_cwt(x, ('gmw', {}))[0])
+    assert np.array_equal(a, b)
+
+
+def test_input_kinds_and_streams(sb):
+    x = chirp_signal(3000, seed=1).astype(np.float32)
+    ref = _np(sb.ssq_cwt(x, 'morlet')[0])
+    xt = torch.as_tensor(x).cuda()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        out = sb.ssq_cwt(xt, 'morlet')[0]
+    s.synchronize()
+    assert np.array_equal(_np(out), ref)
+    out_np = sb.ssq_cwt(x, 'morlet', astensor=False)
+    assert isinstance(out_np[0], np.ndarray) and np.array_equal(out_np[0], ref)
+
+
+def test_nan_inputs_are_zeroed(sb):
+    x = chirp_signal(500, seed=2)
+    y = x.copy()
+    y[[3, 100]] = np.nan
+    y[7] = np.inf
+    z = x.copy()
+    z[[3, 100, 7]] = 0
+    a = _np(sb.ssq_cwt(y, 'morlet')[0])
+    b = _np(sb.ssq_cwt(z, 'morlet')[0])
+    assert np.array_equal(a, b)
