@@ -104,12 +104,12 @@ def oracle_step(x, scales, f_asc, const):
     return O.ssq_cwt(x, 'gmw_l1', (3., 60.), scales, f_asc, const)
 
 
-def host_params():
+def host_params(N=N_SIG):
     from ssqueezepy_b200 import _params as P
     w = P.Wavelet(WAVELET)
-    sc, st, na, nv = P.process_scales('log-piecewise', N_SIG, w, nv=32,
+    sc, st, na, nv = P.process_scales('log-piecewise', N, w, nv=32,
                                       get_params=True)
-    f = P.compute_associated_frequencies(sc, N_SIG, w, st, 'peak', True, 1., 'cwt')
+    f = P.compute_associated_frequencies(sc, N, w, st, 'peak', True, 1., 'cwt')
     const = P.squeeze_weights(sc, st, nv, 'cwt')
     return w, sc.ravel(), f, const, na
 
@@ -163,8 +163,8 @@ def run_ours(args):
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
     lib = L.load()
-    w, sc, f, const, na = host_params()
-    N = N_SIG
+    N = args.n
+    w, sc, f, const, na = host_params(N)
     Npad, n1, _ = P.p2up(N)
     x_np = chirp_signal(N, seed=rank).astype(np.float32)
     x = torch.as_tensor(x_np, device=dev)
@@ -176,7 +176,7 @@ def run_ours(args):
     sc_d = torch.as_tensor(sc, dtype=torch.float64, device=dev)
     cst_d = torch.as_tensor(const, dtype=torch.float64, device=dev)
     kind, *wp = w.kernel_params()
-    cw = L.make_wavelet(kind, wp)
+    cw = L.make_wavelet(kind, wp, w.band())
     mode, bp = P.bin_params(f, True)
     cb = L.make_bins(mode, bp, na, True)
     gamma = 10 * P.EPS32
@@ -225,6 +225,22 @@ def run_ours(args):
     value = world * N / (step_ms_max * 1e-3)
 
     # end to end through the public API from pinned host memory
+    e2e_value = None
+    if args.no_e2e:
+        pass
+    else:
+        e2e_value = run_e2e(sb, torch, dist, x_np, na, N, st, world, dev, barrier,
+                            args)
+    if rank == 0:
+        emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
+             launches, clocks, sc, f, const, Tx, Wx)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(sb, torch, dist, x_np, na, N, st, world, dev, barrier, args):
     x_pin = torch.from_numpy(x_np).pin_memory()
     Tx_pin = torch.empty((na, N), dtype=torch.complex64).pin_memory()
     for _ in range(2):
@@ -243,10 +259,13 @@ def run_ours(args):
                           device=dev)
     if world > 1:
         dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e_value = world * N / (float(e2e_ms.item()) * 1e-3)
+    return world * N / (float(e2e_ms.item()) * 1e-3)
 
-    if rank == 0:
-        hbm, src = peaks()
+
+def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
+         launches, clocks, sc, f, const, Tx, Wx):
+    hbm, src = peaks()
+    if True:
         alg_cwt = (4 + 8 * na) * N          # read x, write Wx
         alg_total = (4 + 16 * na) * N       # read x, write Wx and Tx
         cwt_avg = float(np.mean(cwt_ms))
@@ -259,8 +278,9 @@ def run_ours(args):
             "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "ssq_cwt N=160000 GMW(3,60) nv=32 log-piecewise "
-                                   "(293 rows) float32 reflect, one signal per GPU",
+            "config": {"workload": "ssq_cwt N=%d GMW(3,60) nv=32 log-piecewise "
+                                   "(%d rows) float32 reflect, one signal per GPU"
+                                   % (N, na),
                        "N": N, "na": na, "Npad": Npad, "batch_per_gpu": 1,
                        "l2": "252 MB buffer written between timed steps",
                        "parallelism": "dp%d" % world},
@@ -269,8 +289,9 @@ def run_ours(args):
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": None, "peak_source": src,
                          "path_frac": alg_total / (step_ms_max * 1e-3) / 1e9 / hbm},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * N,
-                    "d2h_bytes_per_step": 8 * na * N},
+            "e2e": (None if e2e_value is None else
+                    {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * N,
+                     "d2h_bytes_per_step": 8 * na * N}),
             "gpu_launches": launches * args.steps,
             "clocks": clocks,
         }
@@ -280,16 +301,13 @@ def run_ours(args):
             tc = time.perf_counter() - t0
             line["cpu_baseline"] = {
                 "value": N / tc, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                "sample": "one full N=160,000 ssq_cwt, float64 numpy/scipy restatement"}
+                "sample": "one full N=%d ssq_cwt, float64 numpy/scipy restatement, "
+                          "scipy.fft workers=%d" % (N, os.cpu_count())}
             Tg, Wg = Tx[0].cpu().numpy(), Wx[0].cpu().numpy()
             line["parity"] = {
                 "Wx_rel_l2": float(np.linalg.norm(Wg - Wo) / np.linalg.norm(Wo)),
                 "Tx_rel_l2": float(np.linalg.norm(Tg - To) / np.linalg.norm(To))}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
 
 
 def main():
@@ -300,6 +318,10 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu', action='store_true',
                     help='skip the CPU baseline / parity leg')
+    ap.add_argument('--no-e2e', action='store_true',
+                    help='skip the end-to-end (host buffers) leg')
+    ap.add_argument('--n', type=int, default=N_SIG,
+                    help='signal length (default 160000; smaller for profiling)')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)

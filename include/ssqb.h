@@ -55,11 +55,14 @@ enum { SSQB_F32 = 0, SSQB_F64 = 1 };
 /* Frequency-domain wavelet (wavelets.py:498-530, _gmw.py:187-251).
  * kind 0 Morlet:   p = {mu, ks = exp(-mu^2/2), C1 = sqrt(2) cs pi^(1/4), 0}
  * kind 1 GMW L1:   p = {gamma, beta, wc = (beta/gamma)^(1/gamma), log(wc)}
- * kind 2 GMW L2:   p = {gamma, beta, wc, sqrt(2 pi gamma 2^r / Gamma(r))} */
+ * kind 2 GMW L2:   p = {gamma, beta, wc, sqrt(2 pi gamma 2^r / Gamma(r))}
+ * band = {w_lo, w_hi}: psih is taken as 0 outside [w_lo, w_hi] (where it is
+ * below ~1e-30 of its peak); band[0] >= band[1] evaluates everywhere. */
 typedef struct ssqb_wavelet {
   int32_t kind;
   int32_t reserved;
   double p[4];
+  double band[2];
 } ssqb_wavelet;
 
 /* Bin mapping of the squeeze (algos.py:81-87, 356-374).

@@ -22,7 +22,7 @@ PADTYPES = {'zero': 0, 'reflect': 1, 'symmetric': 2, 'replicate': 3, 'wrap': 4}
 
 class CWavelet(ctypes.Structure):
     _fields_ = [('kind', ctypes.c_int32), ('reserved', ctypes.c_int32),
-                ('p', ctypes.c_double * 4)]
+                ('p', ctypes.c_double * 4), ('band', ctypes.c_double * 2)]
 
 
 class CBins(ctypes.Structure):
@@ -107,11 +107,12 @@ def ptr(t):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 
 
-def make_wavelet(kind, p):
+def make_wavelet(kind, p, band=(0., 0.)):
     w = CWavelet()
     w.kind = int(kind)
     for i, v in enumerate(p):
         w.p[i] = float(v)
+    w.band[0], w.band[1] = float(band[0]), float(band[1])
     return w
 
 

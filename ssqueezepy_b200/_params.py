@@ -250,6 +250,32 @@ class Wavelet():
                 psih[..., n // 2] /= 2
         return psih
 
+    def band(self, log_floor=-69.):
+        """(w_lo, w_hi): outside this interval |psih(w)| < e^log_floor times
+        its peak (e^-69 ~ 1e-30), so the kernels skip evaluating it there."""
+        k = self.constants()
+        if self.kind == self.KIND_MORLET:
+            mu = k['mu']
+            r = np.sqrt(-2 * log_floor)
+            neg = np.sqrt(max(0., -2 * log_floor - mu**2))
+            return (min(mu - r, -neg), mu + r)
+        g, b, wc = k['gamma'], k['beta'], k['wc']
+
+        def e(w):  # log of psih relative to its peak at wc
+            return b * np.log(w / wc) - (w**g - wc**g)
+        lo, hi = 1e-300, wc
+        for _ in range(200):
+            mid = np.sqrt(lo * hi)
+            lo, hi = (mid, hi) if e(mid) < log_floor else (lo, mid)
+        w_lo = lo
+        lo, hi = wc, wc * 2
+        while e(hi) > log_floor:
+            hi *= 2
+        for _ in range(200):
+            mid = .5 * (lo + hi)
+            lo, hi = (mid, hi) if e(mid) > log_floor else (lo, mid)
+        return (w_lo, hi)
+
     def kernel_params(self):
         """(kind, p0, p1, p2, p3) passed to the CUDA kernels."""
         k = self.constants()

@@ -165,7 +165,7 @@ def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
     ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     sc_d = _on_device(sp, 'scales', dev)
     kind, *wp = wavelet.kernel_params()
-    cw = L.make_wavelet(kind, wp)
+    cw = L.make_wavelet(kind, wp, wavelet.band())
     cb = L.make_bins(*ssq) if ssq is not None else None
     gamma = _default_gamma(dtype) if gamma is None else gamma
     with torch.cuda.device(dev):

@@ -89,6 +89,8 @@ static int check_wavelet(const ssqb_wavelet* w, WavDev* out) {
   out->kind = w->kind;
   out->p0 = w->p[0]; out->p1 = w->p[1]; out->p2 = w->p[2]; out->p3 = w->p[3];
   out->wcg = (w->kind == 1) ? std::pow(w->p[2], w->p[0]) : 0.0;
+  out->lo = w->band[0];
+  out->hi = w->band[1];
   if (w->kind != 0 && !(w->p[0] > 0 && w->p[1] > 0))
     return fail(SSQB_EINVAL, "GMW gamma and beta must be positive");
   return SSQB_OK;

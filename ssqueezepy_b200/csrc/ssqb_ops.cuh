@@ -11,6 +11,7 @@ struct WavDev {
   int kind;          // 0 Morlet, 1 GMW L1 (bandpass), 2 GMW L2 (energy)
   double p0, p1, p2, p3;  // Morlet: mu, ks, C1; GMW: gamma, beta, wc, wcl | l2norm
   double wcg;        // GMW: wc^gamma
+  double lo, hi;     // psih = 0 outside [lo, hi] (skipped when lo >= hi)
 };
 
 struct BinDev {
@@ -59,6 +60,7 @@ __device__ __forceinline__ int pad_src(long long q, int N, int padtype) {
 
 // ---- wavelets, float64 (wavelets.py:521-527, _gmw.py:203-210, 246-251) --
 __device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
+  if (w.lo < w.hi && (x < w.lo || x > w.hi)) return 0.0;
   if (w.kind == 0) {
     const double d = x - w.p0;
     const double a = -0.5 * (d * d);

@@ -41,6 +41,7 @@ tile_single(Op op, Tables tb) {
   const int b = blockIdx.z;
   const int row0 = blockIdx.x * NF;
   const int nrows = op.rows();
+  int nz = 0;
   for (int e = threadIdx.x; e < TILE; e += kNT) {
     const int f = e >> LOGL, k = e & (L - 1);
     C v[NARR];
@@ -51,10 +52,13 @@ tile_single(Op op, Tables tb) {
       for (int a = 0; a < NARR; ++a) v[a] = mk((typename RealOf<C>::type)0, (typename RealOf<C>::type)0);
     }
 #pragma unroll
-    for (int a = 0; a < NARR; ++a) buf[a][spad(e)] = v[a];
+    for (int a = 0; a < NARR; ++a) {
+      buf[a][spad(e)] = v[a];
+      nz |= (v[a].x != 0) | (v[a].y != 0);
+    }
   }
-  __syncthreads();
-  fft_tile<C, LOGL, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
+  // a tile whose input is all zero transforms to zero: skip the stages
+  if (__syncthreads_or(nz)) fft_tile<C, LOGL, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
   for (int e = threadIdx.x; e < TILE; e += kNT) {
     int f, n;
     if (Op::kStoreRowFast) { f = e % NF; n = e / NF; }
@@ -81,15 +85,18 @@ tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_
   const int b = blockIdx.z;
   const int row = row_lo + blockIdx.y;
   const int k1_0 = blockIdx.x * NF;
+  int nz = 0;
   for (int e = threadIdx.x; e < TILE; e += kNT) {
     const int f = e % NF, k2 = e / NF;
     C v[NARR];
     op.load(b, row, k1_0 + f + L1 * k2, v);
 #pragma unroll
-    for (int a = 0; a < NARR; ++a) buf[a][spad(f * L2 + k2)] = v[a];
+    for (int a = 0; a < NARR; ++a) {
+      buf[a][spad(f * L2 + k2)] = v[a];
+      nz |= (v[a].x != 0) | (v[a].y != 0);
+    }
   }
-  __syncthreads();
-  fft_tile<C, LOGL2, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
+  if (__syncthreads_or(nz)) fft_tile<C, LOGL2, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
   const size_t L = size_t(1) << log2L;
   C* zrow = Z + (size_t(b) * rows_in_tile + blockIdx.y) * NARR * L;
   for (int e = threadIdx.x; e < TILE; e += kNT) {
@@ -122,14 +129,17 @@ tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo, int
   const int n2_0 = blockIdx.x * NF;
   const size_t L = size_t(1) << log2L;
   const C* zrow = Z + (size_t(b) * rows_in_tile + blockIdx.y) * NARR * L;
+  int nz = 0;
   for (int e = threadIdx.x; e < TILE; e += kNT) {
     const int f = e >> LOGL1, k1 = e & (L1 - 1);
 #pragma unroll
-    for (int a = 0; a < NARR; ++a)
-      buf[a][spad(e)] = zrow[a * L + size_t(n2_0 + f) * L1 + k1];
+    for (int a = 0; a < NARR; ++a) {
+      const C v = zrow[a * L + size_t(n2_0 + f) * L1 + k1];
+      buf[a][spad(e)] = v;
+      nz |= (v.x != 0) | (v.y != 0);
+    }
   }
-  __syncthreads();
-  fft_tile<C, LOGL1, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
+  if (__syncthreads_or(nz)) fft_tile<C, LOGL1, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
   for (int e = threadIdx.x; e < TILE; e += kNT) {
     const int f = e % NF, n1 = e / NF;
     op.store(b, row, L2 * n1 + n2_0 + f, buf, f * L1 + n1, f * L1);

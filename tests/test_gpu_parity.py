@@ -166,7 +166,9 @@ def _full_size(sb, N, wk, sqf, dtype):
     wav = P.Wavelet((nm, dict(opts, dtype=dtype)))
     Tx, Wx, f, s = sb.ssq_cwt(x, wav, scales='log-piecewise', nv=32,
                               ssq_freqs=sqf)
-    return x, _np(Tx), _np(Wx), np.asarray(f), _np(s).astype(np.float64)
+    s64 = P.process_scales('log-piecewise', N, wav, nv=32).ravel()
+    assert np.array_equal(s64.astype(np.float32), _np(s))
+    return x, _np(Tx), _np(Wx), np.asarray(f), s64
 
 
 @pytest.mark.parametrize('N, wk, sqf', [(10000, 'morlet6', 'log'),
