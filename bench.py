@@ -183,13 +183,17 @@ def run_ours(args):
     st = torch.cuda.current_stream()
     sp = L.stream_ptr(st)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
-    launches = lib.ssqb_cwt_launches(1, Npad, na, L.F32, wsb) + 1
+    # float32 data, float64 arithmetic (the default of the public API)
+    prec = L.F32X if args.arith == 'float64' else L.F32
+    wsb = max(wsb, lib.ssqb_cwt_workspace_bytes(1, N, Npad, na, prec))
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    launches = lib.ssqb_cwt_launches(1, Npad, na, prec, wsb) + 1
 
-    def step(ev=None):
+    def step(ev=None, prec=prec):
         if ev:
             ev[0].record(st)
         L.check(lib.ssqb_cwt(L.ptr(x), 1, N, Npad, n1, 1, 0, L.ptr(sc_d), na, cw, 1.0,
-                             cb, gamma, L.F32, L.ptr(Wx), None, None, L.ptr(idx),
+                             cb, gamma, prec, L.ptr(Wx), None, None, L.ptr(idx),
                              L.ptr(ws), wsb, sp), 'cwt')
         if ev:
             ev[1].record(st)
@@ -281,6 +285,7 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
             "config": {"workload": "ssq_cwt N=%d GMW(3,60) nv=32 log-piecewise "
                                    "(%d rows) float32 reflect, one signal per GPU"
                                    % (N, na),
+                       "arithmetic": args.arith,
                        "N": N, "na": na, "Npad": Npad, "batch_per_gpu": 1,
                        "l2": "252 MB buffer written between timed steps",
                        "parallelism": "dp%d" % world},
@@ -320,6 +325,8 @@ def main():
                     help='skip the CPU baseline / parity leg')
     ap.add_argument('--no-e2e', action='store_true',
                     help='skip the end-to-end (host buffers) leg')
+    ap.add_argument('--arith', default='float64', choices=['float64', 'float32'],
+                    help='arithmetic inside the transforms (data stay float32)')
     ap.add_argument('--n', type=int, default=N_SIG,
                     help='signal length (default 160000; smaller for profiling)')
     args = ap.parse_args()

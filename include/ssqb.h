@@ -47,7 +47,11 @@ enum {
   SSQB_EWORKSPACE = 4     /* workspace smaller than required */
 };
 
-enum { SSQB_F32 = 0, SSQB_F64 = 1 };
+/* precision: SSQB_F32 float32 data and arithmetic; SSQB_F64 float64 data
+ * and arithmetic; SSQB_F32X float32 data (x, Wx, Sx, Tx, w) with float64
+ * arithmetic inside the transforms, so bin decisions match the float64 path
+ * except at exact ties. */
+enum { SSQB_F32 = 0, SSQB_F64 = 1, SSQB_F32X = 2 };
 
 /* padtype: 0 zero, 1 reflect, 2 symmetric, 3 replicate, 4 wrap
  * (utils/common.py:54-158) */

@@ -8,7 +8,7 @@ include/ssqb.h). Host code only derives float64 parameters (scales,
 frequencies, bin mapping); there is no CPU fallback.
 """
 from ._transforms import (cwt, ssq_cwt, icwt, stft, ssq_stft, ssqueeze,
-                          phase_cwt, phase_stft, Wavelet)
+                          phase_cwt, phase_stft, Wavelet, configure)
 from ._params import (p2up, process_scales, make_scales, cwt_scalebounds,
                       center_frequency, adm_ssq, logscale_transition_idx,
                       infer_scaletype, nv_from_scales)
@@ -16,7 +16,7 @@ from . import _lib
 
 __version__ = '0.1.0'
 __all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
-           'phase_cwt', 'phase_stft', 'Wavelet', 'p2up', 'process_scales',
+           'phase_cwt', 'phase_stft', 'Wavelet', 'configure', 'p2up', 'process_scales',
            'make_scales', 'cwt_scalebounds', 'center_frequency', 'adm_ssq',
            'logscale_transition_idx', 'infer_scaletype', 'nv_from_scales']
 

@@ -14,7 +14,7 @@ import torch
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, '_lib', 'libssqb.so')
 
-F32, F64 = 0, 1
+F32, F64, F32X = 0, 1, 2
 OK, EINVAL, EUNSUPPORTED, ECUDA, EWORKSPACE = 0, 1, 2, 3, 4
 NO_BIN = 0xFFFF
 PADTYPES = {'zero': 0, 'reflect': 1, 'symmetric': 2, 'replicate': 3, 'wrap': 4}

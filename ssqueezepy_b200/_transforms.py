@@ -10,6 +10,8 @@ runs in the CUDA kernels of libssqb.so (through `_lib`). Inputs may be numpy
 arrays or torch tensors (CPU or CUDA); outputs are CUDA tensors
 (`astensor=True`, the default) or numpy arrays.
 """
+import os
+
 import numpy as np
 import torch
 
@@ -17,7 +19,7 @@ from . import _lib as L
 from . import _params as P
 
 __all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
-           'phase_cwt', 'phase_stft', 'Wavelet']
+           'phase_cwt', 'phase_stft', 'Wavelet', 'configure']
 
 Wavelet = P.Wavelet
 
@@ -65,8 +67,29 @@ def _out(t, astensor, is_2d=True):
     return t.cpu().numpy()
 
 
+# Arithmetic of float32 transforms: 'float64' (default) computes the FFTs,
+# phase transform and bins in float64 and stores float32, so bins match the
+# float64 path; 'float32' is faster and matches the reference's own float32
+# path in accuracy (Tx differs from float64 at ~1e-3 relative L2 through bin
+# flips).
+_CONFIG = {'float32_arithmetic': os.environ.get('SSQB_FLOAT32_ARITHMETIC',
+                                                'float64')}
+
+
+def configure(float32_arithmetic=None):
+    """Set the arithmetic of float32 transforms ('float64' or 'float32');
+    returns the current settings."""
+    if float32_arithmetic is not None:
+        if float32_arithmetic not in ('float64', 'float32'):
+            raise ValueError("`float32_arithmetic` must be 'float64' or 'float32'")
+        _CONFIG['float32_arithmetic'] = float32_arithmetic
+    return dict(_CONFIG)
+
+
 def _prec(dtype):
-    return L.F64 if dtype == 'float64' else L.F32
+    if dtype == 'float64':
+        return L.F64
+    return L.F32 if _CONFIG['float32_arithmetic'] == 'float32' else L.F32X
 
 
 def _default_gamma(dtype):

@@ -12,8 +12,8 @@ namespace ssqb {
 // Twiddle tables and the status word live in module memory (no cudaMalloc).
 static __device__ double2 g_tw_lo[1 << TW_SPLIT];
 static __device__ double2 g_tw_hi[1 << (TW_LOG - TW_SPLIT)];
-static __device__ float2 g_tw4k_f[4096];
-static __device__ double2 g_tw4k_d[4096];
+static __device__ float2 g_seg_f[SEG_SIZE];
+static __device__ double2 g_seg_d[SEG_SIZE];
 static __device__ int g_status;
 
 __global__ void init_tables_kernel() {
@@ -28,11 +28,13 @@ __global__ void init_tables_kernel() {
     sincospi((double)t / (double)(1 << (TW_LOG - TW_SPLIT - 1)), &s, &c);
     g_tw_hi[t] = make_double2(c, s);
   }
-  if (t < 4096) {  // exp(2 pi i t / 4096)
+  if (t >= 2 && t < SEG_SIZE) {  // segment M = 2^floor(log2 t): exp(2 pi i (t-M) / M)
+    int M = 1;
+    while ((M << 1) <= t) M <<= 1;
     double s, c;
-    sincospi((double)t / 2048.0, &s, &c);
-    g_tw4k_d[t] = make_double2(c, s);
-    g_tw4k_f[t] = make_float2((float)c, (float)s);
+    sincospi(2.0 * (double)(t - M) / (double)M, &s, &c);
+    g_seg_d[t] = make_double2(c, s);
+    g_seg_f[t] = make_float2((float)c, (float)s);
   }
   if (t == 0) g_status = 0;
 }
@@ -64,13 +66,13 @@ static int get_tables(Tables* out) {
     t.tw_lo = (const double2*)p;
     if ((e = cudaGetSymbolAddress(&p, g_tw_hi))) return cuda_fail(e, "symbol tw_hi");
     t.tw_hi = (const double2*)p;
-    if ((e = cudaGetSymbolAddress(&p, g_tw4k_f))) return cuda_fail(e, "symbol tw4k_f");
-    t.tw4k_f = (const float2*)p;
-    if ((e = cudaGetSymbolAddress(&p, g_tw4k_d))) return cuda_fail(e, "symbol tw4k_d");
-    t.tw4k_d = (const double2*)p;
+    if ((e = cudaGetSymbolAddress(&p, g_seg_f))) return cuda_fail(e, "symbol seg_f");
+    t.seg_f = (const float2*)p;
+    if ((e = cudaGetSymbolAddress(&p, g_seg_d))) return cuda_fail(e, "symbol seg_d");
+    t.seg_d = (const double2*)p;
     if ((e = cudaGetSymbolAddress(&p, g_status))) return cuda_fail(e, "symbol status");
     t.status = (int*)p;
-    init_tables_kernel<<<16, 256>>>();
+    init_tables_kernel<<<SEG_SIZE / 256, 256>>>();
     if ((e = cudaGetLastError())) return cuda_fail(e, "init tables");
     if ((e = cudaDeviceSynchronize())) return cuda_fail(e, "init tables sync");
     g_tables[dev] = t;
@@ -112,14 +114,24 @@ static int check_bins(const ssqb_bins* b, int na, BinDev* out) {
   return SSQB_OK;
 }
 
-static size_t csize(int precision) { return precision == SSQB_F64 ? 16 : 8; }
+// bytes of one complex value of the transform arithmetic
+static size_t csize(int precision) { return precision == SSQB_F32 ? 8 : 16; }
+static bool valid_precision(int p) { return p == SSQB_F32 || p == SSQB_F64 || p == SSQB_F32X; }
+// storage precision of data arrays: F32X stores float32
+static int data_prec(int p) { return p == SSQB_F32X ? SSQB_F32 : p; }
 
 static size_t xhat_bytes(int B, int Npad) { return (size_t)B * Npad * sizeof(double2); }
 
+static bool cwt_two_pass(int m, int precision) {
+  return precision == SSQB_F32 ? two_pass<float2>(m) : two_pass<double2>(m);
+}
+
+// intermediate needed for one row: the float64 x_hat (if it takes two
+// passes) and the CWT (if it does)
 static size_t min_z_bytes(int B, int Npad, int precision) {
-  if (!two_pass(ilog2i(Npad))) return 0;
-  const size_t a = (size_t)B * Npad * sizeof(double2);
-  const size_t c = (size_t)B * 2 * Npad * csize(precision);
+  const int m = ilog2i(Npad);
+  const size_t a = two_pass<double2>(m) ? (size_t)B * Npad * sizeof(double2) : 0;
+  const size_t c = cwt_two_pass(m, precision) ? (size_t)B * 2 * Npad * csize(precision) : 0;
   return a > c ? a : c;
 }
 
@@ -151,8 +163,8 @@ int ssqb_device_status(void* stream, int* status_out) {
 size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
   (void)N;
   if (B < 1 || Npad < 1 || na < 1) return 0;
-  size_t z = 0;
-  if (two_pass(ilog2i(Npad))) {
+  size_t z = min_z_bytes(B, Npad, precision);
+  if (cwt_two_pass(ilog2i(Npad), precision)) {
     const size_t per_row = (size_t)B * 2 * Npad * csize(precision);
     size_t rows = ((size_t)48 << 20) / per_row;
     if (rows < 1) rows = 1;
@@ -167,12 +179,13 @@ size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
 int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_bytes) {
   if (B < 1 || na < 1 || !is_pow2(Npad)) return -1;
   const int m = ilog2i(Npad);
-  if (!two_pass(m)) return 2;
+  const int nx = two_pass<double2>(m) ? 2 : 1;
+  if (!cwt_two_pass(m, precision)) return nx + 1;
   const size_t xb = xhat_bytes(B, Npad);
   if (workspace_bytes < xb) return -1;
   const size_t zcap = (workspace_bytes - xb) / csize(precision);
   const int S = rows_per_tile(zcap, B, 2, m, na);
-  return 2 + 2 * ((na + S - 1) / S);
+  return nx + 2 * ((na + S - 1) / S);
 }
 
 int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
@@ -182,8 +195,8 @@ int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpa
              void* workspace, size_t workspace_bytes, void* stream) {
   if (!x || !scales || !Wx || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
-  if (precision != SSQB_F32 && precision != SSQB_F64)
-    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
   if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
     return fail(SSQB_EUNSUPPORTED, "Npad must be a power of two in [8, 2^22]");
   if (Npad < N || n1 < 0 || n1 + N > Npad) return fail(SSQB_EINVAL, "bad padding geometry");
@@ -210,7 +223,7 @@ int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpa
   unsigned char* zb = (unsigned char*)workspace + xhat_bytes(B, Npad);
   const size_t zbytes = workspace_bytes - xhat_bytes(B, Npad);
   int e;
-  if (precision == SSQB_F32)
+  if (data_prec(precision) == SSQB_F32)
     e = run_xhat_f32((const float*)x, B, N, Npad, n1, padtype, xh, (double2*)zb,
                      zbytes / sizeof(double2), tb, st);
   else
@@ -225,6 +238,11 @@ int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpa
                      (float)(1.0 / Npad), gamma, (float2*)Wx, (float2*)dWx, (float*)w,
                      idx, tb.status};
     e = run_cwt_f32(op, B, m, (float2*)zb, zbytes / sizeof(float2), tb, st);
+  } else if (precision == SSQB_F32X) {
+    CwtOp<double2, float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,
+                              1.0 / Npad, gamma, (float2*)Wx, (float2*)dWx, (float*)w,
+                              idx, tb.status};
+    e = run_cwt_f32x(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st);
   } else {
     CwtOp<double2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt, 1.0 / Npad,
                       gamma, (double2*)Wx, (double2*)dWx, (double*)w, idx, tb.status};
@@ -240,8 +258,9 @@ static int squeeze_common(const void* Wx, int kind, const void* src, const doubl
   if (!Wx || !src || !cst || !Tx) return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
   if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
-  if (precision != SSQB_F32 && precision != SSQB_F64)
-    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  precision = data_prec(precision);
   if (nbins < 1 || nbins > 65535) return fail(SSQB_EINVAL, "nbins must be in [1, 65535]");
   BinDev bd{};
   if (kind != 0) {
@@ -249,7 +268,7 @@ static int squeeze_common(const void* Wx, int kind, const void* src, const doubl
     if (r) return r;
   }
   const size_t smem = (size_t)nbins * 32 * csize(precision) +
-                      (size_t)na * (precision == SSQB_F64 ? 8 : 4);
+                      (size_t)na * (precision == SSQB_F64 ? 8 : 4);  // data precision
   if (smem > 227 * 1024)
     return fail(SSQB_EUNSUPPORTED, "too many bins for the shared-memory squeeze");
   Tables tb;
@@ -298,8 +317,8 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
   if (!is_pow2(n_fft) || n_fft < 8 || n_fft > 4096)
     return fail(SSQB_EUNSUPPORTED, "n_fft must be a power of two in [8, 4096]");
   if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
-  if (precision != SSQB_F32 && precision != SSQB_F64)
-    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
   const int nrow = n_fft / 2 + 1;
   BinDev bd{};
   if (idx) {
@@ -320,6 +339,12 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
                              n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
                              (float2*)Sx, (float2*)dSx, (float*)w, idx, tb.status};
     e = run_stft_f32(op, B, m, tb, st);
+  } else if (precision == SSQB_F32X) {
+    StftOp<float, double2, float2> op{(const float*)x, window, diff_window, Sfs, bd, N,
+                                      n_fft, hop, n1, padtype, s21, modulated ? 1 : 0,
+                                      nframes, gamma, (float2*)Sx, (float2*)dSx, (float*)w,
+                                      idx, tb.status};
+    e = run_stft_f32x(op, B, m, tb, st);
   } else {
     StftOp<double, double2> op{(const double*)x, window, diff_window, Sfs, bd, N, n_fft,
                                hop, n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
@@ -336,8 +361,9 @@ int ssqb_icwt(const void* Wx, const double* row_weights, const double* x_mean,
   if (!Wx || !row_weights || !x) return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
   if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
-  if (precision != SSQB_F32 && precision != SSQB_F64)
-    return fail(SSQB_EINVAL, "precision must be SSQB_F32 or SSQB_F64");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  precision = data_prec(precision);
   int e = run_icwt(Wx, row_weights, x_mean, mean_weight, B, na, N, precision, x,
                    (cudaStream_t)stream);
   if (e) return cuda_fail((cudaError_t)e, "icwt launch");

@@ -1,60 +1,94 @@
-// Shared-memory Stockham FFT over a tile of NF independent sequences of
-// length L = 2^LOGL (NF * L = TILE elements per array), NARR arrays
-// transformed together (they share twiddles), radix 16/8/4/2 butterflies in
+// Shared-memory Stockham FFT over a tile of NF independent rows of length
+// L = 2^LOGL, NARR arrays transformed together (they share twiddles and,
+// at the ends, the prologue / epilogue), butterflies of radix <= RMAX in
 // registers. Stockham autosort formulation (Govindaraju et al., "High
 // performance discrete Fourier transforms on graphics processors", SC 2008):
-// stage with radix R after NS = prod(previous radices):
+// a stage of radix R after NS = product of the previous radices maps
 //   v[r] = x[j + r*L/R] * w_{NS*R}^{r*(j mod NS)},  v = DFT_R(v),
 //   y[(j div NS)*NS*R + (j mod NS) + r*NS] = v[r].
-// Each stage loads into registers, syncs, then stores in place.
+//
+// The first stage reads its inputs straight from the caller's loader and the
+// last stage (optionally) hands its outputs straight to the caller's storer,
+// so only the L/R-strided exchanges between stages go through shared memory.
+// Rows are XOR-swizzled in groups of G = 128 B / sizeof(C) elements and
+// padded to a stride chosen so that both row-fastest and column-fastest
+// thread mappings hit distinct banks.
 #pragma once
 #include "ssqb_common.cuh"
 
 namespace ssqb {
 
-// one spare slot per 16 elements: stride-R stores hit distinct banks
-__host__ __device__ __forceinline__ constexpr int spad(int p) { return p + (p >> 4); }
-__host__ __device__ constexpr int spad_size(int n) { return n + (n >> 4); }
+template <typename C> struct FftCfg;
+template <> struct FftCfg<float2> {
+  static constexpr int TILE = 4096, RMAX_LOG = 4, G_LOG = 4;
+};
+template <> struct FftCfg<double2> {
+  static constexpr int TILE = 2048, RMAX_LOG = 3, G_LOG = 3;
+};
 
-// radix schedule for 2^m: radix-16 stages, finishing with 8 and/or 4
-__host__ __device__ constexpr int fft_nstages(int m) {
-  return m <= 4 ? 1 : (m % 4 == 0 ? m / 4 : m / 4 + 1);
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// radix schedule: ceil(m / RMAX_LOG) stages, radices as even as possible,
+// larger ones first
+__host__ __device__ constexpr int fft_nstages(int m, int rmax_log) {
+  return m <= rmax_log ? 1 : cdiv(m, rmax_log);
 }
-__host__ __device__ constexpr int fft_rlog(int m, int s) {
-  if (m <= 4) return m;
-  int a = m / 4, r = m % 4;
-  if (r == 0) return 4;
-  if (r == 1) return s < a - 1 ? 4 : (s == a - 1 ? 3 : 2);
-  if (r == 2) return s < a ? 4 : 2;
-  return s < a ? 4 : 3;
+__host__ __device__ constexpr int fft_rlog(int m, int rmax_log, int s) {
+  const int n = fft_nstages(m, rmax_log);
+  const int q = m / n, rem = m % n;
+  return s < rem ? q + 1 : q;
 }
-__host__ __device__ constexpr int fft_lns(int m, int s) {
+__host__ __device__ constexpr int fft_lns(int m, int rmax_log, int s) {
   int l = 0;
-  for (int q = 0; q < s; ++q) l += fft_rlog(m, q);
+  for (int t = 0; t < s; ++t) l += fft_rlog(m, rmax_log, t);
   return l;
 }
 
-// cos / sin of a*pi/8
-__host__ __device__ constexpr double cos16(int a) {
-  constexpr double C1 = 0.92387953251128675613, C3 = 0.38268343236508977173,
-                   H = 0.70710678118654752440;
-  const double t[16] = {1.0, C1, H, C3, 0.0, -C3, -H, -C1,
-                        -1.0, -C1, -H, -C3, 0.0, C3, H, C1};
-  return t[a & 15];
+// row stride: L plus an offset d so that f*LP covers distinct bank groups
+// for f in [0, min(NF, G)) while the in-row swizzle handles the rest
+__host__ __device__ constexpr int row_pitch(int L, int NF, int G) {
+  return L + (NF >= G ? 1 : (NF == 1 ? 0 : G / NF));
 }
-__host__ __device__ constexpr double sin16(int a) { return cos16(a - 4); }
 
-// v *= exp(SIGN*2*pi*i*a/16); `a` folds to a constant once loops unroll
+template <typename C, int LOGL, int NF>
+struct Layout {
+  static constexpr int L = 1 << LOGL;
+  static constexpr int G = 1 << FftCfg<C>::G_LOG;
+  static constexpr int LP = row_pitch(L, NF, G);
+  static constexpr int ARR = NF * LP;  // elements per array
+  __device__ __forceinline__ static int at(int f, int m) {
+    return f * LP + (m ^ ((m >> FftCfg<C>::G_LOG) & (G - 1)));
+  }
+};
+
+// cos / sin of a*pi/16 (a in 0..31)
+__host__ __device__ constexpr double cos32(int a) {
+  const double t[32] = {
+      1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+      0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173,
+      0.19509032201612826785, 0.0, -0.19509032201612826785, -0.38268343236508977173,
+      -0.55557023301960222474, -0.70710678118654752440, -0.83146961230254523708,
+      -0.92387953251128675613, -0.98078528040323044913, -1.0, -0.98078528040323044913,
+      -0.92387953251128675613, -0.83146961230254523708, -0.70710678118654752440,
+      -0.55557023301960222474, -0.38268343236508977173, -0.19509032201612826785, 0.0,
+      0.19509032201612826785, 0.38268343236508977173, 0.55557023301960222474,
+      0.70710678118654752440, 0.83146961230254523708, 0.92387953251128675613,
+      0.98078528040323044913};
+  return t[a & 31];
+}
+__host__ __device__ constexpr double sin32(int a) { return cos32(a - 8); }
+
+// v *= exp(SIGN*2*pi*i*a/32); `a` folds to a constant once loops unroll
 template <int SIGN, typename C>
-__device__ __forceinline__ C rot16(C v, int a) {
+__device__ __forceinline__ C rot32(C v, int a) {
   typedef typename RealOf<C>::type T;
-  a &= 15;
+  a &= 31;
   if (a == 0) return v;
-  if (a == 4) return cmul_i<SIGN>(v);
-  if (a == 8) return mk(-v.x, -v.y);
-  if (a == 12) return cmul_i<-SIGN>(v);
-  const T c = (T)cos16(a);
-  const T s = (T)(SIGN * sin16(a));
+  if (a == 8) return cmul_i<SIGN>(v);
+  if (a == 16) return mk(-v.x, -v.y);
+  if (a == 24) return cmul_i<-SIGN>(v);
+  const T c = (T)cos32(a);
+  const T s = (T)(SIGN * sin32(a));
   return mk(v.x * c - v.y * s, v.x * s + v.y * c);
 }
 
@@ -64,71 +98,113 @@ template <int R> __host__ __device__ constexpr int bitrev(int x) {
   return r;
 }
 
-template <int R, int SIGN, typename C, int LEN>
-__device__ __forceinline__ void dft_level(C (&v)[R]) {
+template <int R, int SIGN, int LEN, typename C>
+__device__ __forceinline__ void dft_level(C (&t)[R]) {
   constexpr int half = LEN / 2;
 #pragma unroll
   for (int b0 = 0; b0 < R; b0 += LEN) {
 #pragma unroll
     for (int j = 0; j < half; ++j) {
-      C u = v[b0 + j];
-      C t = rot16<SIGN>(v[b0 + j + half], j * (16 / LEN));
-      v[b0 + j] = cadd(u, t);
-      v[b0 + j + half] = csub(u, t);
+      const C u = t[b0 + j];
+      const C w = rot32<SIGN>(t[b0 + j + half], j * (32 / LEN));
+      t[b0 + j] = cadd(u, w);
+      t[b0 + j + half] = csub(u, w);
     }
   }
 }
 
-// In-register DFT of size R (2, 4, 8, 16), sign SIGN, natural order in/out.
+// In-register DFT of size R (2..16), sign SIGN, natural order in and out
+// (radix-2 decimation in time over bit-reversed inputs).
 template <int R, int SIGN, typename C>
 __device__ __forceinline__ void dft(C (&v)[R]) {
   C t[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) t[i] = v[bitrev<R>(i)];
-  if constexpr (R >= 2) dft_level<R, SIGN, C, 2>(t);
-  if constexpr (R >= 4) dft_level<R, SIGN, C, 4>(t);
-  if constexpr (R >= 8) dft_level<R, SIGN, C, 8>(t);
-  if constexpr (R >= 16) dft_level<R, SIGN, C, 16>(t);
+  if constexpr (R >= 2) dft_level<R, SIGN, 2>(t);
+  if constexpr (R >= 4) dft_level<R, SIGN, 4>(t);
+  if constexpr (R >= 8) dft_level<R, SIGN, 8>(t);
+  if constexpr (R >= 16) dft_level<R, SIGN, 16>(t);
 #pragma unroll
   for (int i = 0; i < R; ++i) v[i] = t[i];
 }
 
-template <typename C, int LOGL, int NF, int NT, int SIGN, int NARR, int S>
-__device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __restrict__ tw4k) {
+// Thread mappings of butterfly items to (row f, column j in [0, L/R)).
+enum { MAP_J = 0, MAP_F = 1 };
+template <int MAP, int NF, int LR>
+__device__ __forceinline__ void item_fj(int it, int& f, int& j) {
+  if (MAP == MAP_J) { f = it >> LR; j = it & ((1 << LR) - 1); }
+  else { f = it % NF; j = it / NF; }
+}
+
+// Twiddle segment table: seg[M + m] = exp(2 pi i m / M), M = 2..4096.
+template <typename C> __device__ __forceinline__ const C* seg_table(const Tables& t);
+template <> __device__ __forceinline__ const float2* seg_table<float2>(const Tables& t) {
+  return t.seg_f;
+}
+template <> __device__ __forceinline__ const double2* seg_table<double2>(const Tables& t) {
+  return t.seg_d;
+}
+
+// One full transform of the tile.
+//   ld(f, m, C (&v)[NARR])   input element m of row f (all arrays)
+//   st(f, m, C (&v)[NARR])   output element m of row f (when DIRECT_OUT)
+// buf: NARR arrays of Layout::ARR elements. MAP_IN / MAP_OUT: mappings of the
+// first and last stage; middle stages use MAP_J. With DIRECT_OUT == false the
+// last stage writes shared memory (read it back with Layout::at after the
+// function returns; it ends with __syncthreads()).
+template <typename C, int LOGL, int NF, int NT, int SIGN, int NARR, int MAP_IN, int MAP_OUT,
+          bool DIRECT_OUT, int S, class LD, class ST>
+__device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __restrict__ seg,
+                                          const LD& ld, const ST& st) {
+  typedef Layout<C, LOGL, NF> LY;
+  constexpr int RL_MAX = FftCfg<C>::RMAX_LOG;
+  constexpr int NSTG = fft_nstages(LOGL, RL_MAX);
   constexpr int L = 1 << LOGL;
-  constexpr int RL = fft_rlog(LOGL, S);
+  constexpr int RL = fft_rlog(LOGL, RL_MAX, S);
   constexpr int R = 1 << RL;
-  constexpr int LNS = fft_lns(LOGL, S);
+  constexpr int LNS = fft_lns(LOGL, RL_MAX, S);
   constexpr int NS = 1 << LNS;
-  constexpr int NB = NF * L / R;
-  constexpr int PER = (NB + NT - 1) / NT;
-  constexpr int LR = LOGL - RL;  // log2(L/R)
+  constexpr int LR = LOGL - RL;
+  constexpr int NB = NF * (L / R);
+  constexpr int PER = cdiv(NB, NT);
+  constexpr bool FIRST = (S == 0), LAST = (S == NSTG - 1);
+  constexpr int MAP = FIRST ? MAP_IN : (LAST ? MAP_OUT : MAP_J);
   const int tid = threadIdx.x;
   C v[NARR][PER][R];
+  // gather
 #pragma unroll
   for (int p = 0; p < PER; ++p) {
-    const int bb = tid + p * NT;
-    if (NB % NT == 0 || bb < NB) {
-      const int f = bb >> LR;
-      const int j = bb & ((L / R) - 1);
+    const int it = tid + p * NT;
+    if (NB % NT == 0 || it < NB) {
+      int f, j;
+      item_fj<MAP, NF, LR>(it, f, j);
 #pragma unroll
-      for (int a = 0; a < NARR; ++a)
+      for (int r = 0; r < R; ++r) {
+        if constexpr (FIRST) {
+          C t[NARR];
+          ld(f, j + r * (L / R), t);
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[a][p][r] = buf[a][spad(f * L + j + r * (L / R))];
+          for (int a = 0; a < NARR; ++a) v[a][p][r] = t[a];
+        } else {
+#pragma unroll
+          for (int a = 0; a < NARR; ++a) v[a][p][r] = buf[a][LY::at(f, j + r * (L / R))];
+        }
+      }
     }
   }
-  __syncthreads();
+  if constexpr (!FIRST && !(LAST && DIRECT_OUT)) __syncthreads();
+  // twiddle, butterfly, scatter
 #pragma unroll
   for (int p = 0; p < PER; ++p) {
-    const int bb = tid + p * NT;
-    if (NB % NT == 0 || bb < NB) {
-      const int f = bb >> LR;
-      const int j = bb & ((L / R) - 1);
+    const int it = tid + p * NT;
+    if (NB % NT == 0 || it < NB) {
+      int f, j;
+      item_fj<MAP, NF, LR>(it, f, j);
       const int k = j & (NS - 1);
-      if constexpr (S > 0) {
+      if constexpr (!FIRST) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          C w = __ldg(tw4k + ((r * k) << (12 - LNS - RL)));
+          C w = __ldg(seg + NS * R + r * k);
           if (SIGN < 0) w.y = -w.y;
 #pragma unroll
           for (int a = 0; a < NARR; ++a) v[a][p][r] = cmul(v[a][p][r], w);
@@ -136,23 +212,32 @@ __device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __rest
       }
 #pragma unroll
       for (int a = 0; a < NARR; ++a) dft<R, SIGN>(v[a][p]);
-      const int base = f * L + ((j >> LNS) << (LNS + RL)) + k;
+      const int base = ((j >> LNS) << (LNS + RL)) + k;
 #pragma unroll
-      for (int a = 0; a < NARR; ++a)
+      for (int r = 0; r < R; ++r) {
+        if constexpr (LAST && DIRECT_OUT) {
+          C t[NARR];
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[a][spad(base + r * NS)] = v[a][p][r];
+          for (int a = 0; a < NARR; ++a) t[a] = v[a][p][r];
+          st(f, base + r * NS, t);
+        } else {
+#pragma unroll
+          for (int a = 0; a < NARR; ++a) buf[a][LY::at(f, base + r * NS)] = v[a][p][r];
+        }
+      }
     }
   }
-  __syncthreads();
+  if constexpr (!(LAST && DIRECT_OUT)) __syncthreads();
+  if constexpr (!LAST)
+    fft_stage<C, LOGL, NF, NT, SIGN, NARR, MAP_IN, MAP_OUT, DIRECT_OUT, S + 1>(buf, seg, ld,
+                                                                             st);
 }
 
-// Full transform of the tile; caller must __syncthreads() after filling.
-template <typename C, int LOGL, int NF, int NT, int SIGN, int NARR, int S = 0>
-__device__ __forceinline__ void fft_tile(C* const (&buf)[NARR], const C* __restrict__ tw4k) {
-  if constexpr (S < fft_nstages(LOGL)) {
-    fft_stage<C, LOGL, NF, NT, SIGN, NARR, S>(buf, tw4k);
-    fft_tile<C, LOGL, NF, NT, SIGN, NARR, S + 1>(buf, tw4k);
-  }
+template <typename C, int LOGL, int NF, int NT, int SIGN, int NARR, int MAP_IN, int MAP_OUT,
+          bool DIRECT_OUT, class LD, class ST>
+__device__ __forceinline__ void fft_rows(C* const (&buf)[NARR], const C* __restrict__ seg,
+                                         const LD& ld, const ST& st) {
+  fft_stage<C, LOGL, NF, NT, SIGN, NARR, MAP_IN, MAP_OUT, DIRECT_OUT, 0>(buf, seg, ld, st);
 }
 
 }  // namespace ssqb

@@ -1,5 +1,5 @@
 // Tile-FFT kernel instantiations for x_hat and the fused CWT, and their
-// host launchers (single pass for Npad <= 4096, else two passes).
+// host launchers (one pass when Npad fits a tile, else two passes).
 #include "launch.h"
 
 namespace ssqb {
@@ -12,9 +12,9 @@ static cudaError_t prep(K kernel, size_t smem) {
 
 template <class Op, typename C, int SIGN, int LOGL>
 static int launch_single(const Op& op, int B, int nrows, const Tables& tb, cudaStream_t st) {
-  constexpr int NF = kTile / (1 << LOGL);
-  const size_t smem = (size_t)Op::NARR * spad_size(kTile) * sizeof(C);
-  auto k = tile_single<Op, C, LOGL, kTile, SIGN>;
+  constexpr int NF = tile_of<C>() / (1 << LOGL);
+  const size_t smem = tile_smem<C>(Op::NARR, LOGL);
+  auto k = tile_single<Op, C, LOGL, SIGN>;
   cudaError_t e = prep(k, smem);
   if (e) return e;
   dim3 grid((nrows + NF - 1) / NF, 1, B);
@@ -25,11 +25,11 @@ static int launch_single(const Op& op, int B, int nrows, const Tables& tb, cudaS
 template <class Op, typename C, int SIGN, int LOGL2>
 static int launch_p1(const Op& op, int B, int log2L, C* Z, int row_lo, int rows,
                      const Tables& tb, cudaStream_t st) {
-  const size_t smem = (size_t)Op::NARR * spad_size(kTile) * sizeof(C);
-  auto k = tile_pass1<Op, C, LOGL2, kTile, SIGN>;
+  const size_t smem = tile_smem<C>(Op::NARR, LOGL2);
+  auto k = tile_pass1<Op, C, LOGL2, SIGN>;
   cudaError_t e = prep(k, smem);
   if (e) return e;
-  dim3 grid((1u << log2L) / kTile, rows, B);
+  dim3 grid((1u << log2L) / tile_of<C>(), rows, B);
   k<<<grid, kNT, smem, st>>>(op, tb, Z, log2L, row_lo, rows);
   return cudaGetLastError();
 }
@@ -37,36 +37,41 @@ static int launch_p1(const Op& op, int B, int log2L, C* Z, int row_lo, int rows,
 template <class Op, typename C, int SIGN, int LOGL1>
 static int launch_p2(const Op& op, int B, int log2L, const C* Z, int row_lo, int rows,
                      const Tables& tb, cudaStream_t st) {
-  const size_t smem = (size_t)Op::NARR * spad_size(kTile) * sizeof(C);
-  auto k = tile_pass2<Op, C, LOGL1, kTile, SIGN>;
+  const size_t smem = tile_smem<C>(Op::NARR, LOGL1);
+  auto k = tile_pass2<Op, C, LOGL1, SIGN>;
   cudaError_t e = prep(k, smem);
   if (e) return e;
-  dim3 grid((1u << log2L) / kTile, rows, B);
+  dim3 grid((1u << log2L) / tile_of<C>(), rows, B);
   k<<<grid, kNT, smem, st>>>(op, tb, Z, log2L, row_lo, rows);
   return cudaGetLastError();
 }
 
-#define SSQB_SINGLE_CASES(OP, C, SIGN)                                      \
-  switch (log2L) {                                                          \
-    case 3: return launch_single<OP, C, SIGN, 3>(op, B, nrows, tb, st);    \
-    case 4: return launch_single<OP, C, SIGN, 4>(op, B, nrows, tb, st);    \
-    case 5: return launch_single<OP, C, SIGN, 5>(op, B, nrows, tb, st);    \
-    case 6: return launch_single<OP, C, SIGN, 6>(op, B, nrows, tb, st);    \
-    case 7: return launch_single<OP, C, SIGN, 7>(op, B, nrows, tb, st);    \
-    case 8: return launch_single<OP, C, SIGN, 8>(op, B, nrows, tb, st);    \
-    case 9: return launch_single<OP, C, SIGN, 9>(op, B, nrows, tb, st);    \
-    case 10: return launch_single<OP, C, SIGN, 10>(op, B, nrows, tb, st);  \
-    case 11: return launch_single<OP, C, SIGN, 11>(op, B, nrows, tb, st);  \
-    case 12: return launch_single<OP, C, SIGN, 12>(op, B, nrows, tb, st);  \
-    default: return (int)cudaErrorInvalidValue;                            \
+template <class Op, typename C, int SIGN>
+static int run_single(const Op& op, int B, int nrows, int log2L, const Tables& tb,
+                      cudaStream_t st) {
+  switch (log2L) {
+    case 3: return launch_single<Op, C, SIGN, 3>(op, B, nrows, tb, st);
+    case 4: return launch_single<Op, C, SIGN, 4>(op, B, nrows, tb, st);
+    case 5: return launch_single<Op, C, SIGN, 5>(op, B, nrows, tb, st);
+    case 6: return launch_single<Op, C, SIGN, 6>(op, B, nrows, tb, st);
+    case 7: return launch_single<Op, C, SIGN, 7>(op, B, nrows, tb, st);
+    case 8: return launch_single<Op, C, SIGN, 8>(op, B, nrows, tb, st);
+    case 9: return launch_single<Op, C, SIGN, 9>(op, B, nrows, tb, st);
+    case 10: return launch_single<Op, C, SIGN, 10>(op, B, nrows, tb, st);
+    case 11: return launch_single<Op, C, SIGN, 11>(op, B, nrows, tb, st);
+    case 12:
+      if constexpr (tile_of<C>() >= 4096)
+        return launch_single<Op, C, SIGN, 12>(op, B, nrows, tb, st);
+      else
+        return (int)cudaErrorInvalidValue;
+    default: return (int)cudaErrorInvalidValue;
   }
+}
 
 template <class Op, typename C, int SIGN>
 static int run_tile(const Op& op, int B, int nrows, int log2L, C* Z, size_t zcap,
                     const Tables& tb, cudaStream_t st) {
-  if (!two_pass(log2L)) {
-    SSQB_SINGLE_CASES(Op, C, SIGN)
-  }
+  if (!two_pass<C>(log2L)) return run_single<Op, C, SIGN>(op, B, nrows, log2L, tb, st);
   if (log2L > 22) return (int)cudaErrorInvalidValue;
   const int l2 = log2L / 2, l1 = log2L - l2;
   const int S = rows_per_tile(zcap, B, Op::NARR, log2L, nrows);
@@ -84,6 +89,7 @@ static int run_tile(const Op& op, int B, int nrows, int log2L, C* Z, size_t zcap
     }
     if (e) return e;
     switch (l1) {
+      case 6: e = launch_p2<Op, C, SIGN, 6>(op, B, log2L, Z, r0, rows, tb, st); break;
       case 7: e = launch_p2<Op, C, SIGN, 7>(op, B, log2L, Z, r0, rows, tb, st); break;
       case 8: e = launch_p2<Op, C, SIGN, 8>(op, B, log2L, Z, r0, rows, tb, st); break;
       case 9: e = launch_p2<Op, C, SIGN, 9>(op, B, log2L, Z, r0, rows, tb, st); break;
@@ -118,6 +124,12 @@ int run_cwt_f32(const CwtOp<float2>& op, int B, int log2L, float2* Z, size_t zca
 int run_cwt_f64(const CwtOp<double2>& op, int B, int log2L, double2* Z, size_t zcap,
                 const Tables& tb, cudaStream_t st) {
   return run_tile<CwtOp<double2>, double2, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
+}
+
+int run_cwt_f32x(const CwtOp<double2, float2>& op, int B, int log2L, double2* Z,
+                 size_t zcap, const Tables& tb, cudaStream_t st) {
+  return run_tile<CwtOp<double2, float2>, double2, 1>(op, B, op.na, log2L, Z, zcap, tb,
+                                                       st);
 }
 
 }  // namespace ssqb

@@ -17,9 +17,11 @@ inline int rows_per_tile(size_t zcap_elems, int B, int narr, int log2L, int nrow
   return (int)s;
 }
 
-// single-pass when L <= 4096; else two passes with log2(L2) = m/2
-constexpr int kTile = 4096;
-inline bool two_pass(int log2L) { return log2L > 12; }
+// single pass when L fits one tile (4096 float2 / 2048 double2 elements);
+// else two passes with log2(L2) = m/2
+template <typename C> inline bool two_pass(int log2L) {
+  return (1 << log2L) > FftCfg<C>::TILE;
+}
 
 int run_xhat_f32(const float* x, int B, int N, int Npad, int n1, int padtype,
                  double2* xh, double2* Z, size_t zcap, const Tables& tb,
@@ -31,10 +33,14 @@ int run_cwt_f32(const CwtOp<float2>& op, int B, int log2L, float2* Z, size_t zca
                 const Tables& tb, cudaStream_t st);
 int run_cwt_f64(const CwtOp<double2>& op, int B, int log2L, double2* Z, size_t zcap,
                 const Tables& tb, cudaStream_t st);
+int run_cwt_f32x(const CwtOp<double2, float2>& op, int B, int log2L, double2* Z,
+                 size_t zcap, const Tables& tb, cudaStream_t st);
 int run_stft_f32(const StftOp<float, float2>& op, int B, int log2L,
                  const Tables& tb, cudaStream_t st);
 int run_stft_f64(const StftOp<double, double2>& op, int B, int log2L,
                  const Tables& tb, cudaStream_t st);
+int run_stft_f32x(const StftOp<float, double2, float2>& op, int B, int log2L,
+                  const Tables& tb, cudaStream_t st);
 
 // squeeze; src_kind 0 = uint16 index, 1 = phase from dWx (cwt or stft), 2 = w
 int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, const double* sfs,

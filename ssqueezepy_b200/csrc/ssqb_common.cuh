@@ -38,21 +38,18 @@ template <> __device__ __forceinline__ double2 to_c<double2>(double2 v) { return
 
 // Twiddle tables. The unit root exp(2*pi*i*e / 2^22) for e in [0, 2^22) is
 // tw_hi[e >> 11] * tw_lo[e & 2047], both tables double precision (filled by
-// sincospi in double on the device). tw4k holds exp(2*pi*i*m/4096) directly,
-// rounded once, in float and double.
+// sincospi in double on the device). seg_f / seg_d hold, for each power of
+// two M = 2..4096, the M roots exp(2*pi*i*m/M) at [M, 2M), rounded once.
 constexpr int TW_LOG = 22;
 constexpr int TW_SPLIT = 11;
+constexpr int SEG_SIZE = 8192;
 struct Tables {
   const double2* tw_lo;   // 2048
   const double2* tw_hi;   // 2048
-  const float2* tw4k_f;   // 4096
-  const double2* tw4k_d;  // 4096
+  const float2* seg_f;    // SEG_SIZE
+  const double2* seg_d;   // SEG_SIZE
   int* status;            // device status word (0 = ok)
 };
-
-template <typename C> __device__ __forceinline__ const C* tw4k(const Tables& t);
-template <> __device__ __forceinline__ const float2* tw4k<float2>(const Tables& t) { return t.tw4k_f; }
-template <> __device__ __forceinline__ const double2* tw4k<double2>(const Tables& t) { return t.tw4k_d; }
 
 // exp(SIGN * 2*pi*i * e / 2^log2n), e in [0, 2^log2n), log2n <= 22, computed
 // in double from the two-level table.

@@ -136,7 +136,7 @@ template <> __device__ __forceinline__ void put_w<double2>(double2* p, double v)
 template <typename TX>
 struct XhatOp {
   static constexpr int NARR = 1;
-  static constexpr bool kStoreRowFast = false;
+  static constexpr bool kDirect = true;
   const TX* x;       // (B, N)
   double2* xh;       // (B, Npad)
   int N, Npad, n1, padtype;
@@ -145,17 +145,27 @@ struct XhatOp {
     const int s = pad_src((long long)k - n1, N, padtype);
     v[0] = make_double2(s >= 0 ? (double)x[(size_t)b * N + s] : 0.0, 0.0);
   }
-  __device__ void store(int b, int, int n, double2* const (&seq)[1], int pos, int) const {
-    xh[(size_t)b * Npad + n] = seq[0][spad(pos)];
+  __device__ void store(int b, int, int n, double2 (&v)[1]) const {
+    xh[(size_t)b * Npad + n] = v[0];
   }
 };
 
 // ---- fused CWT ---------------------------------------------------------------
-template <typename C>
+// C: arithmetic type of the transform; OC: stored type of Wx / dWx / w.
+template <typename OC> __device__ __forceinline__ OC out_c(double2 v);
+template <> __device__ __forceinline__ float2 out_c<float2>(double2 v) {
+  return make_float2((float)v.x, (float)v.y);
+}
+template <> __device__ __forceinline__ double2 out_c<double2>(double2 v) { return v; }
+template <typename OC> __device__ __forceinline__ OC out_c(float2 v);
+template <> __device__ __forceinline__ float2 out_c<float2>(float2 v) { return v; }
+
+template <typename C, typename OC = C>
 struct CwtOp {
   typedef typename RealOf<C>::type T;
+  typedef typename RealOf<OC>::type OT;
   static constexpr int NARR = 2;
-  static constexpr bool kStoreRowFast = false;
+  static constexpr bool kDirect = true;
   const double2* xh;      // (B, Npad) float64
   const double* scales;   // (na)
   WavDev wav;
@@ -165,9 +175,9 @@ struct CwtOp {
   double inv_dt;
   T inv_npad;
   double gamma;
-  C* Wx;                  // (B, na, N)
-  C* dWx;                 // optional
-  T* w;                   // optional phase transform
+  OC* Wx;                 // (B, na, N)
+  OC* dWx;                // optional
+  OT* w;                  // optional phase transform
   uint16_t* idx;          // optional bin index
   int* status;
   __device__ int rows() const { return na; }
@@ -182,31 +192,33 @@ struct CwtOp {
     v[0] = to_c<C>(y);
     v[1] = to_c<C>(make_double2(-y.y * c, y.x * c));
   }
-  __device__ void store(int b, int row, int n, C* const (&seq)[2], int pos, int) const {
+  __device__ void store(int b, int row, int n, C (&v)[2]) const {
     const int j = n - n1;
     if (j < 0 || j >= N) return;
-    C Wv = seq[0][spad(pos)], dWv = seq[1][spad(pos)];
+    C Wv = v[0], dWv = v[1];
     Wv.x *= inv_npad; Wv.y *= inv_npad;
     dWv.x *= inv_npad; dWv.y *= inv_npad;
     const size_t o = ((size_t)b * na + row) * N + j;
-    if (Wx) Wx[o] = Wv;
-    if (dWx) dWx[o] = dWv;
+    if (Wx) Wx[o] = out_c<OC>(Wv);
+    if (dWx) dWx[o] = out_c<OC>(dWv);
     if (idx || w) {
+      // bins from the arithmetic-precision values, before output rounding
       double wv;
       const uint16_t k = phase_bin(Wv, dWv, 0.0, false, bins, gamma, status,
                                    w ? &wv : nullptr);
       if (idx) idx[o] = k;
-      if (w) w[o] = (T)wv;
+      if (w) w[o] = (OT)wv;
     }
   }
 };
 
 // ---- fused STFT (modulated framing, stft_utils.py:69-98; _stft.py:127-147)
-template <typename TX, typename C>
+template <typename TX, typename C, typename OC = C>
 struct StftOp {
   typedef typename RealOf<C>::type T;
+  typedef typename RealOf<OC>::type OT;
   static constexpr int NARR = 1;
-  static constexpr bool kStoreRowFast = true;
+  static constexpr bool kDirect = false;
   const TX* x;             // (B, N)
   const double* win;       // (n_fft)
   const double* dwin;      // (n_fft), already times fs
@@ -214,9 +226,9 @@ struct StftOp {
   BinDev bins;
   int N, L, hop, n1, padtype, s21, modulated, nframes;
   double gamma;
-  C* Sx;                   // (B, L/2+1, nframes)
-  C* dSx;
-  T* w;
+  OC* Sx;                  // (B, L/2+1, nframes)
+  OC* dSx;
+  OT* w;
   uint16_t* idx;
   int* status;
   __device__ int rows() const { return nframes; }
@@ -227,25 +239,26 @@ struct StftOp {
     const double xv = s >= 0 ? (double)x[(size_t)b * N + s] : 0.0;
     v[0] = to_c<C>(make_double2(xv * __ldg(win + q), xv * __ldg(dwin + q)));
   }
-  __device__ void store(int b, int t, int n, C* const (&seq)[1], int, int rowbase) const {
+  template <class LY>
+  __device__ void store_smem(int b, int t, int n, C* const (&buf)[1], int f) const {
     const int nrow = (L >> 1) + 1;
     if (n >= nrow) return;
-    const C zk = seq[0][spad(rowbase + n)];
-    const C zm = seq[0][spad(rowbase + ((L - n) & (L - 1)))];
+    const C zk = buf[0][LY::at(f, n)];
+    const C zm = buf[0][LY::at(f, (L - n) & (L - 1))];
     const T hf = (T)0.5;
     // z = a + i*b with real a (window) and b (diff window):
     // A_k = (Z_k + conj Z_{L-k}) / 2,  B_k = (Z_k - conj Z_{L-k}) / (2i)
     const C S = mk(hf * (zk.x + zm.x), hf * (zk.y - zm.y));
     const C dS = mk(hf * (zk.y + zm.y), -hf * (zk.x - zm.x));
     const size_t o = ((size_t)b * nrow + n) * nframes + t;
-    if (Sx) Sx[o] = S;
-    if (dSx) dSx[o] = dS;
+    if (Sx) Sx[o] = out_c<OC>(S);
+    if (dSx) dSx[o] = out_c<OC>(dS);
     if (idx || w) {
       double wv;
       const uint16_t k = phase_bin(S, dS, __ldg(sfs + n), true, bins, gamma, status,
                                    w ? &wv : nullptr);
       if (idx) idx[o] = k;
-      if (w) w[o] = (T)wv;
+      if (w) w[o] = (OT)wv;
     }
   }
 };

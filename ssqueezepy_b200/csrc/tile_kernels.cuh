@@ -1,24 +1,22 @@
-// Generic tile-FFT kernels: one pass for L <= 4096 (NF sequences per CTA),
-// or two passes (four-step) for L = L1*L2 through an intermediate buffer.
+// Tile-FFT kernels: one pass for L <= TILE (NF rows per CTA), or two passes
+// (four-step) for L = L1*L2 through an intermediate buffer Z.
 //
 // For the two-pass form, with input index k = k1 + L1*k2 and output index
 // n = L2*n1 + n2 (k1, n1 in [0, L1); k2, n2 in [0, L2)):
 //   y[L2*n1 + n2] = sum_k1 w_L1^(k1*n1) * [ w_L^(k1*n2) *
-//                   sum_k2 Y[k1 + L1*k2] w_L2^(k2*n2) ]           (w = e^(SIGN 2 pi i / .))
+//                   sum_k2 Y[k1 + L1*k2] w_L2^(k2*n2) ]        (w = e^(SIGN 2 pi i / .))
 // pass 1: per k1 a length-L2 transform over k2, times w_L^(k1*n2), stored as
 //         Z[n2][k1];  pass 2: per n2 a length-L1 transform over k1.
 //
 // An `Op` supplies the data at both ends:
-//   Op::NARR                           arrays transformed together
-//   Op::kStoreRowFast                  epilogue iterates rows fastest
-//   op.rows()                          number of rows (sequences) per batch item
-//   op.load(b, row, k, C out[NARR])    input element k of row `row` of item b
-//   op.store(b, row, n, seq, pos, rowbase)
-//                                      output element n; its value in array a
-//                                      is seq[a][spad(pos)]. In the one-pass
-//                                      kernel element m of the same row sits at
-//                                      seq[a][spad(rowbase + m)], so ops may
-//                                      read partners too (e.g. n and L-n)
+//   Op::NARR                             arrays transformed together
+//   Op::kDirect                          true: outputs go straight to op.store
+//   op.rows()                            rows (sequences) per batch item
+//   op.load(b, row, k, C (&v)[NARR])     input element k of row `row`
+//   op.store(b, row, n, C (&v)[NARR])    output element n (kDirect)
+//   op.store_smem<LY>(b, row, n, buf, f) output element n read from shared
+//                                        memory row f (!kDirect; may read
+//                                        partner elements, e.g. L-n)
 #pragma once
 #include "fft_tile.cuh"
 
@@ -26,102 +24,99 @@ namespace ssqb {
 
 constexpr int kNT = 256;  // threads per CTA for all tile kernels
 
-template <class Op, typename C, int LOGL, int TILE, int SIGN>
+template <typename C> __host__ __device__ constexpr int tile_of() {
+  return FftCfg<C>::TILE;
+}
+
+template <class Op, typename C, int LOGL, int SIGN>
 __global__ void __launch_bounds__(kNT)
 tile_single(Op op, Tables tb) {
   constexpr int NARR = Op::NARR;
+  constexpr int TILE = tile_of<C>();
   constexpr int L = 1 << LOGL;
   constexpr int NF = TILE / L;
+  typedef Layout<C, LOGL, NF> LY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* base = reinterpret_cast<C*>(smem_raw);
   C* bufs[NARR];
 #pragma unroll
-  for (int a = 0; a < NARR; ++a) bufs[a] = base + a * spad_size(TILE);
+  for (int a = 0; a < NARR; ++a) bufs[a] = base + a * LY::ARR;
   C* const(&buf)[NARR] = bufs;
   const int b = blockIdx.z;
   const int row0 = blockIdx.x * NF;
   const int nrows = op.rows();
-  int nz = 0;
-  for (int e = threadIdx.x; e < TILE; e += kNT) {
-    const int f = e >> LOGL, k = e & (L - 1);
-    C v[NARR];
+  auto ld = [&](int f, int m, C (&v)[NARR]) {
     if (row0 + f < nrows) {
-      op.load(b, row0 + f, k, v);
+      op.load(b, row0 + f, m, v);
     } else {
 #pragma unroll
-      for (int a = 0; a < NARR; ++a) v[a] = mk((typename RealOf<C>::type)0, (typename RealOf<C>::type)0);
+      for (int a = 0; a < NARR; ++a)
+        v[a] = mk((typename RealOf<C>::type)0, (typename RealOf<C>::type)0);
     }
-#pragma unroll
-    for (int a = 0; a < NARR; ++a) {
-      buf[a][spad(e)] = v[a];
-      nz |= (v[a].x != 0) | (v[a].y != 0);
+  };
+  if constexpr (Op::kDirect) {
+    auto st = [&](int f, int m, C (&v)[NARR]) {
+      if (row0 + f < nrows) op.store(b, row0 + f, m, v);
+    };
+    fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, true>(buf, seg_table<C>(tb), ld, st);
+  } else {
+    auto st = [&](int, int, C (&)[NARR]) {};
+    fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, false>(buf, seg_table<C>(tb), ld, st);
+    for (int e = threadIdx.x; e < TILE; e += kNT) {
+      const int f = e % NF, n = e / NF;  // rows fastest: coalesced (row, n) outputs
+      if (row0 + f < nrows) op.template store_smem<LY>(b, row0 + f, n, buf, f);
     }
-  }
-  // a tile whose input is all zero transforms to zero: skip the stages
-  if (__syncthreads_or(nz)) fft_tile<C, LOGL, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
-  for (int e = threadIdx.x; e < TILE; e += kNT) {
-    int f, n;
-    if (Op::kStoreRowFast) { f = e % NF; n = e / NF; }
-    else { f = e >> LOGL; n = e & (L - 1); }
-    if (row0 + f < nrows) op.store(b, row0 + f, n, buf, f * L + n, f * L);
   }
 }
 
-// pass 1: CTA = (k1 block of NF1 = TILE/L2 columns, row within the row tile,
+// pass 1: CTA = (k1 block of NF = TILE/L2 columns, row within the row tile,
 // batch item). Z layout: [b][row - row_lo][a][n2][k1].
-template <class Op, typename C, int LOGL2, int TILE, int SIGN>
+template <class Op, typename C, int LOGL2, int SIGN>
 __global__ void __launch_bounds__(kNT)
 tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_in_tile) {
   constexpr int NARR = Op::NARR;
+  constexpr int TILE = tile_of<C>();
   constexpr int L2 = 1 << LOGL2;
   constexpr int NF = TILE / L2;
+  typedef Layout<C, LOGL2, NF> LY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* base = reinterpret_cast<C*>(smem_raw);
   C* bufs[NARR];
 #pragma unroll
-  for (int a = 0; a < NARR; ++a) bufs[a] = base + a * spad_size(TILE);
+  for (int a = 0; a < NARR; ++a) bufs[a] = base + a * LY::ARR;
   C* const(&buf)[NARR] = bufs;
   const int L1 = 1 << (log2L - LOGL2);
   const int b = blockIdx.z;
   const int row = row_lo + blockIdx.y;
   const int k1_0 = blockIdx.x * NF;
-  int nz = 0;
-  for (int e = threadIdx.x; e < TILE; e += kNT) {
-    const int f = e % NF, k2 = e / NF;
-    C v[NARR];
-    op.load(b, row, k1_0 + f + L1 * k2, v);
-#pragma unroll
-    for (int a = 0; a < NARR; ++a) {
-      buf[a][spad(f * L2 + k2)] = v[a];
-      nz |= (v[a].x != 0) | (v[a].y != 0);
-    }
-  }
-  if (__syncthreads_or(nz)) fft_tile<C, LOGL2, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
   const size_t L = size_t(1) << log2L;
   C* zrow = Z + (size_t(b) * rows_in_tile + blockIdx.y) * NARR * L;
-  for (int e = threadIdx.x; e < TILE; e += kNT) {
-    const int f = e % NF, n2 = e / NF;
+  auto ld = [&](int f, int m, C (&v)[NARR]) { op.load(b, row, k1_0 + f + L1 * m, v); };
+  auto st = [&](int f, int m, C (&v)[NARR]) {
     const int k1 = k1_0 + f;
-    const uint32_t ex = (uint32_t)(((uint64_t)k1 * (uint64_t)n2) & (L - 1));
+    const uint32_t ex = (uint32_t)(((uint64_t)k1 * (uint64_t)m) & (L - 1));
     const C w = to_c<C>(unit_root<SIGN>(tb, ex, log2L));
 #pragma unroll
-    for (int a = 0; a < NARR; ++a)
-      zrow[a * L + size_t(n2) * L1 + k1] = cmul(buf[a][spad(f * L2 + n2)], w);
-  }
+    for (int a = 0; a < NARR; ++a) zrow[a * L + size_t(m) * L1 + k1] = cmul(v[a], w);
+  };
+  fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
 
-// pass 2: CTA = (n2 block of NF2 = TILE/L1 values, row, batch item).
-template <class Op, typename C, int LOGL1, int TILE, int SIGN>
+// pass 2: CTA = (n2 block of NF = TILE/L1 values, row, batch item).
+template <class Op, typename C, int LOGL1, int SIGN>
 __global__ void __launch_bounds__(kNT)
-tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo, int rows_in_tile) {
+tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo,
+           int rows_in_tile) {
   constexpr int NARR = Op::NARR;
+  constexpr int TILE = tile_of<C>();
   constexpr int L1 = 1 << LOGL1;
   constexpr int NF = TILE / L1;
+  typedef Layout<C, LOGL1, NF> LY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* base = reinterpret_cast<C*>(smem_raw);
   C* bufs[NARR];
 #pragma unroll
-  for (int a = 0; a < NARR; ++a) bufs[a] = base + a * spad_size(TILE);
+  for (int a = 0; a < NARR; ++a) bufs[a] = base + a * LY::ARR;
   C* const(&buf)[NARR] = bufs;
   const int L2 = 1 << (log2L - LOGL1);
   const int b = blockIdx.z;
@@ -129,21 +124,21 @@ tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo, int
   const int n2_0 = blockIdx.x * NF;
   const size_t L = size_t(1) << log2L;
   const C* zrow = Z + (size_t(b) * rows_in_tile + blockIdx.y) * NARR * L;
-  int nz = 0;
-  for (int e = threadIdx.x; e < TILE; e += kNT) {
-    const int f = e >> LOGL1, k1 = e & (L1 - 1);
+  auto ld = [&](int f, int m, C (&v)[NARR]) {
 #pragma unroll
-    for (int a = 0; a < NARR; ++a) {
-      const C v = zrow[a * L + size_t(n2_0 + f) * L1 + k1];
-      buf[a][spad(e)] = v;
-      nz |= (v.x != 0) | (v.y != 0);
-    }
-  }
-  if (__syncthreads_or(nz)) fft_tile<C, LOGL1, NF, kNT, SIGN, NARR>(buf, tw4k<C>(tb));
-  for (int e = threadIdx.x; e < TILE; e += kNT) {
-    const int f = e % NF, n1 = e / NF;
-    op.store(b, row, L2 * n1 + n2_0 + f, buf, f * L1 + n1, f * L1);
-  }
+    for (int a = 0; a < NARR; ++a) v[a] = zrow[a * L + size_t(n2_0 + f) * L1 + m];
+  };
+  auto st = [&](int f, int m, C (&v)[NARR]) { op.store(b, row, L2 * m + n2_0 + f, v); };
+  fft_rows<C, LOGL1, NF, kNT, SIGN, NARR, MAP_J, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
+}
+
+// shared memory of one tile kernel: NARR arrays of NF rows at the row pitch
+template <typename C>
+inline size_t tile_smem(int narr, int logl) {
+  const int L = 1 << logl;
+  const int NF = FftCfg<C>::TILE / L;
+  const int G = 1 << FftCfg<C>::G_LOG;
+  return (size_t)narr * NF * row_pitch(L, NF, G) * sizeof(C);
 }
 
 }  // namespace ssqb
