@@ -110,7 +110,8 @@ def host_params(N=N_SIG):
     sc, st, na, nv = P.process_scales('log-piecewise', N, w, nv=32,
                                       get_params=True)
     f = P.compute_associated_frequencies(sc, N, w, st, 'peak', True, 1., 'cwt')
-    const = P.squeeze_weights(sc, st, nv, 'cwt')
+    _, st_a, _, nv_a = P.process_scales(sc, N, get_params=True)  # per-row nv
+    const = P.squeeze_weights(sc, st_a, nv_a, 'cwt')
     return w, sc.ravel(), f, const, na
 
 
@@ -170,7 +171,8 @@ def run_ours(args):
     x = torch.as_tensor(x_np, device=dev)
     Wx = torch.empty((1, na, N), dtype=torch.complex64, device=dev)
     Tx = torch.empty_like(Wx)
-    idx = torch.empty((1, na, N), dtype=torch.uint16, device=dev)
+    ipitch = L.idx_pitch(N)
+    idx = torch.empty((1, na, ipitch), dtype=torch.uint16, device=dev)
     wsb = lib.ssqb_cwt_workspace_bytes(1, N, Npad, na, L.F32)
     ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     sc_d = torch.as_tensor(sc, dtype=torch.float64, device=dev)
@@ -194,11 +196,11 @@ def run_ours(args):
             ev[0].record(st)
         L.check(lib.ssqb_cwt(L.ptr(x), 1, N, Npad, n1, 1, 0, L.ptr(sc_d), na, cw, 1.0,
                              cb, gamma, prec, L.ptr(Wx), None, None, L.ptr(idx),
-                             L.ptr(ws), wsb, sp), 'cwt')
+                             ipitch, L.ptr(ws), wsb, sp), 'cwt')
         if ev:
             ev[1].record(st)
-        L.check(lib.ssqb_squeeze(L.ptr(Wx), L.ptr(idx), L.ptr(cst_d), 1, na, N, na,
-                                 L.F32, L.ptr(Tx), sp), 'squeeze')
+        L.check(lib.ssqb_squeeze(L.ptr(Wx), L.ptr(idx), ipitch, L.ptr(cst_d), 1, na, N,
+                                 na, L.F32, L.ptr(Tx), sp), 'squeeze')
         if ev:
             ev[2].record(st)
 

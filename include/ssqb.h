@@ -88,8 +88,8 @@ SSQB_API int ssqb_version(void);
 SSQB_API const char* ssqb_last_error(void);
 
 /* Copy and clear the device status word of the current device (0 = ok,
- * 1 = bin index out of range, 2 = padded index out of range); synchronizes
- * `stream`. */
+ * 1 = bin index out of range, 2 = padded index out of range, 3 = a bounded
+ * wait on an asynchronous copy expired); synchronizes `stream`. */
 SSQB_API int ssqb_device_status(void* stream, int* status_out);
 
 /* Workspace bytes for ssqb_cwt: the float64 padded-signal spectrum plus
@@ -107,23 +107,24 @@ SSQB_API int ssqb_cwt_launches(int B, int Npad, int na, int precision,
  *   scales (na) double, device
  *   Wx     (B, na, N) complex, required; dWx optional (NULL)
  *   w      (B, na, N) real phase transform, optional (inf where |Wx|<gamma)
- *   idx    (B, na, N) uint16 bin of each entry, 0xFFFF where |Wx|<=gamma;
- *          optional (needs `bins`)
+ *   idx    (B, na, idx_pitch) uint16 bin of each entry, 0xFFFF where
+ *          |Wx|<=gamma; optional (needs `bins`); idx_pitch >= N columns (0 = N;
+ *          a multiple of 32 lets ssqb_squeeze use its bulk-copy kernel)
  * Npad is the padded length (a power of two, 8 <= Npad <= 2^22) and n1 the
  * left pad; dt = 1/fs. rpadded != 0 writes all Npad columns (outputs
  * (B, na, Npad), _cwt.py:293-306 with rpadded=True). */
 SSQB_API int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
              const double* scales, int na, const ssqb_wavelet* wavelet, double dt,
              const ssqb_bins* bins, double gamma, int precision,
-             void* Wx, void* dWx, void* w, uint16_t* idx,
+             void* Wx, void* dWx, void* w, uint16_t* idx, int idx_pitch,
              void* workspace, size_t workspace_bytes, void* stream);
 
 /* Squeeze from a bin index: Tx[b, idx, j] += Wx[b, i, j] * row_weights[i]
- * over i ascending (algos.py:859-984 accumulation order). Tx (B, nbins, N)
- * is overwritten. */
-SSQB_API int ssqb_squeeze(const void* Wx, const uint16_t* idx, const double* row_weights,
-                 int B, int na, int N, int nbins, int precision, void* Tx,
-                 void* stream);
+ * over i ascending (algos.py:859-984 accumulation order). idx rows have
+ * idx_pitch columns (0 = N). Tx (B, nbins, N) is overwritten. */
+SSQB_API int ssqb_squeeze(const void* Wx, const uint16_t* idx, int idx_pitch,
+                          const double* row_weights, int B, int na, int N, int nbins,
+                          int precision, void* Tx, void* stream);
 
 /* Squeeze computing the phase transform on the fly from Wx and dWx
  * (ssqueeze_fast, algos.py:126-150). Sfs (na) non-NULL selects the STFT
@@ -147,7 +148,7 @@ SSQB_API int ssqb_indexed_sum(const void* Wx, const void* w, const double* row_w
 SSQB_API int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padtype,
               int modulated, const double* window, const double* diff_window,
               const double* Sfs, const ssqb_bins* bins, double gamma, int precision,
-              void* Sx, void* dSx, void* w, uint16_t* idx, void* stream);
+              void* Sx, void* dSx, void* w, uint16_t* idx, int idx_pitch, void* stream);
 
 /* One-integral inverse CWT as a weighted row sum (_cwt.py:479-482 with the
  * scaling of :441-452): x[b, j] = sum_i Re(Wx[b, i, j]) * row_weights[i]

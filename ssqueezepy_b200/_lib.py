@@ -40,14 +40,14 @@ SIGNATURES = {
     'ssqb_cwt_launches': (_i, [_i, _i, _i, _i, _sz]),
     'ssqb_cwt': (_i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _i,
                       ctypes.POINTER(CWavelet), _d, ctypes.POINTER(CBins), _d, _i,
-                      _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
-    'ssqb_squeeze': (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp]),
+                      _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    'ssqb_squeeze': (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _vp]),
     'ssqb_ssqueeze_fast': (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(CBins), _d,
                                 _i, _i, _i, _i, _vp, _vp]),
     'ssqb_indexed_sum': (_i, [_vp, _vp, _vp, ctypes.POINTER(CBins), _i, _i, _i,
                               _i, _vp, _vp]),
     'ssqb_stft': (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp,
-                       ctypes.POINTER(CBins), _d, _i, _vp, _vp, _vp, _vp, _vp]),
+                       ctypes.POINTER(CBins), _d, _i, _vp, _vp, _vp, _vp, _i, _vp]),
     'ssqb_icwt': (_i, [_vp, _vp, _vp, _d, _i, _i, _i, _i, _vp, _vp]),
 }
 
@@ -126,6 +126,12 @@ def make_bins(mode, p, nbins, flipud):
     for i in range(4):
         b.p[i] = float(vals[i])
     return b
+
+
+def idx_pitch(n):
+    """Row pitch of a bin-index buffer: n rounded up to 32 columns (lets the
+    squeeze stream rows with 16-byte bulk copies)."""
+    return (n + 31) // 32 * 32
 
 
 def exported_symbols():

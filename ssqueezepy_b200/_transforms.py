@@ -182,7 +182,8 @@ def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
     Wx = torch.empty((B, na, ncol), dtype=cdt, device=dev)
     dWx = torch.empty_like(Wx) if derivative else None
     w = torch.empty((B, na, ncol), dtype=rdt, device=dev) if want_w else None
-    idx = (torch.empty((B, na, ncol), dtype=torch.uint16, device=dev)
+    ipitch = L.idx_pitch(ncol)
+    idx = (torch.empty((B, na, ipitch), dtype=torch.uint16, device=dev)
            if want_idx else None)
     wsb = L.load().ssqb_cwt_workspace_bytes(B, N, Npad, na, prec)
     ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
@@ -195,10 +196,10 @@ def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
         rc = L.load().ssqb_cwt(
             L.ptr(xd), B, N, Npad, n1, ptype, 1 if (rpadded and padtype) else 0,
             L.ptr(sc_d), na, cw, float(dt), cb, float(gamma), prec,
-            L.ptr(Wx), L.ptr(dWx), L.ptr(w), L.ptr(idx), L.ptr(ws), wsb,
+            L.ptr(Wx), L.ptr(dWx), L.ptr(w), L.ptr(idx), ipitch, L.ptr(ws), wsb,
             L.stream_ptr())
     L.check(rc, 'cwt')
-    return dict(Wx=Wx, dWx=dWx, w=w, idx=idx, scales=scales_np,
+    return dict(Wx=Wx, dWx=dWx, w=w, idx=idx, ipitch=ipitch, scales=scales_np,
                 scaletype=scaletype, nv=nv, na=na, N=N, dt=dt, fs=fs,
                 wavelet=wavelet, dtype=dtype, is_2d=is_2d, dev=dev, B=B,
                 gamma=gamma, sc_d=sc_d)
@@ -283,6 +284,26 @@ def _ssq_freqs_for_cwt(ssq_freqs, scales, N, wavelet, cwt_scaletype, maprange,
     return np.asarray(f, np.float64), st.startswith('log')
 
 
+def _ssq_plan(wavelet, scales, N, nv, ssq_freqs, maprange, padtype, dt, sp=None):
+    """Host parameters of the squeeze of `ssq_cwt`: ascending ssq_freqs, bin
+    mapping and per-row weights (float64, cached)."""
+    sp = sp or _scales_plan(scales, N, wavelet, nv)
+    sc, cwt_st = sp['scales'], sp['scaletype']
+
+    def make():
+        f_asc, logscale = _ssq_freqs_for_cwt(
+            ssq_freqs, sc.reshape(-1, 1), N, wavelet, cwt_st, maprange,
+            padtype is not None, dt)
+        mode, bp = P.bin_params(f_asc, logscale)
+        # ssqueeze re-derives (scaletype, nv) from the scale array, so a
+        # log-piecewise grid gets ln2/nv per row (ssqueezing.py:168-169, 124-128)
+        _, st_a, _, nv_a = P.process_scales(sc.reshape(-1, 1), N, get_params=True)
+        const = P.squeeze_weights(sc, st_a, nv_a, 'cwt')
+        return dict(f_asc=f_asc, mode=mode, bp=bp, const=const)
+    return _plan(('ssq', _wkey(wavelet), N, _akey(scales), nv, _akey(ssq_freqs),
+                  _akey(maprange), padtype is not None, dt), make)
+
+
 def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
             ssq_freqs=None, padtype='reflect', squeezing='sum', maprange='peak',
             difftype='trig', difforder=None, gamma=None, vectorized=True,
@@ -306,15 +327,7 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
     sp = _scales_plan(scales, N, wavelet, nv)
     sc, cwt_st, na, nv_ = sp['scales'], sp['scaletype'], sp['na'], sp['nv']
 
-    def make():
-        f_asc, logscale = _ssq_freqs_for_cwt(
-            ssq_freqs, sc.reshape(-1, 1), N, wavelet, cwt_st, maprange,
-            padtype is not None, dt)
-        mode, bp = P.bin_params(f_asc, logscale)
-        const = P.squeeze_weights(sc, cwt_st, nv_, 'cwt')
-        return dict(f_asc=f_asc, mode=mode, bp=bp, const=const)
-    fp = _plan(('ssq', _wkey(wavelet), N, _akey(scales), nv, _akey(ssq_freqs),
-                _akey(maprange), padtype is not None, dt), make)
+    fp = _ssq_plan(wavelet, scales, N, nv, ssq_freqs, maprange, padtype, dt, sp)
     f_asc = fp['f_asc']
     r = _cwt_core(x, wavelet, scales, nv, fs, t, padtype, False, nan_checks,
                   get_dWx, want_idx=True, want_w=get_w,
@@ -322,8 +335,8 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
     Tx = torch.empty_like(r['Wx'])
     cst = _on_device(fp, 'const', r['dev'])
     with torch.cuda.device(r['dev']):
-        rc = L.load().ssqb_squeeze(L.ptr(r['Wx']), L.ptr(r['idx']), L.ptr(cst),
-                                   r['B'], na, N, na, _prec(r['dtype']),
+        rc = L.load().ssqb_squeeze(L.ptr(r['Wx']), L.ptr(r['idx']), r['ipitch'],
+                                   L.ptr(cst), r['B'], na, N, na, _prec(r['dtype']),
                                    L.ptr(Tx), L.stream_ptr())
     L.check(rc, 'squeeze')
     is2 = r['is_2d']
@@ -543,7 +556,8 @@ def _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
     Sx = torch.empty((B, nrow, nframes), dtype=cdt, device=dev)
     dSx = torch.empty_like(Sx) if derivative else None
     w = torch.empty((B, nrow, nframes), dtype=rdt, device=dev) if want_w else None
-    idx = (torch.empty((B, nrow, nframes), dtype=torch.uint16, device=dev)
+    ipitch = L.idx_pitch(nframes)
+    idx = (torch.empty((B, nrow, ipitch), dtype=torch.uint16, device=dev)
            if want_idx else None)
     dwin_s = dwin * fs if modulated else dwin  # _stft.py:132-135
     wd, dwd, sfd = _dev_f64(win, dev), _dev_f64(dwin_s, dev), _dev_f64(Sfs, dev)
@@ -556,9 +570,10 @@ def _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
                                 L.PADTYPES[padtype], 1 if modulated else 0,
                                 L.ptr(wd), L.ptr(dwd), L.ptr(sfd), cb, float(gamma),
                                 _prec(dtype), L.ptr(Sx), L.ptr(dSx), L.ptr(w),
-                                L.ptr(idx), L.stream_ptr())
+                                L.ptr(idx), ipitch, L.stream_ptr())
     L.check(rc, 'stft')
-    return dict(Sx=Sx, dSx=dSx, w=w, idx=idx, Sfs=Sfs, dtype=dtype, dev=dev,
+    return dict(Sx=Sx, dSx=dSx, w=w, idx=idx, ipitch=ipitch, Sfs=Sfs, dtype=dtype,
+                dev=dev,
                 is_2d=is_2d, B=B, nrow=nrow, nframes=nframes, fs=fs, gamma=gamma)
 
 
@@ -597,8 +612,8 @@ def ssq_stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=Non
     Tx = torch.empty_like(r['Sx'])
     cst = _dev_f64(const, r['dev'])
     with torch.cuda.device(r['dev']):
-        rc = L.load().ssqb_squeeze(L.ptr(r['Sx']), L.ptr(r['idx']), L.ptr(cst),
-                                   r['B'], r['nrow'], r['nframes'], r['nrow'],
+        rc = L.load().ssqb_squeeze(L.ptr(r['Sx']), L.ptr(r['idx']), r['ipitch'],
+                                   L.ptr(cst), r['B'], r['nrow'], r['nframes'], r['nrow'],
                                    _prec(r['dtype']), L.ptr(Tx), L.stream_ptr())
     L.check(rc, 'squeeze')
     is2 = r['is_2d']

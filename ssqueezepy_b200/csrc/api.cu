@@ -191,7 +191,7 @@ int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_b
 int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
              const double* scales, int na, const ssqb_wavelet* wavelet, double dt,
              const ssqb_bins* bins, double gamma, int precision,
-             void* Wx, void* dWx, void* w, uint16_t* idx,
+             void* Wx, void* dWx, void* w, uint16_t* idx, int idx_pitch,
              void* workspace, size_t workspace_bytes, void* stream) {
   if (!x || !scales || !Wx || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
@@ -211,6 +211,9 @@ int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpa
     r = check_bins(bins, na, &bd);
     if (r) return r;
   }
+  if (idx_pitch == 0) idx_pitch = rpadded ? Npad : N;
+  if (idx && idx_pitch < (rpadded ? Npad : N))
+    return fail(SSQB_EINVAL, "idx_pitch smaller than the row length");
   const size_t need = xhat_bytes(B, Npad) + min_z_bytes(B, Npad, precision);
   if (workspace_bytes < need)
     return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
@@ -236,25 +239,27 @@ int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpa
   if (precision == SSQB_F32) {
     CwtOp<float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,
                      (float)(1.0 / Npad), gamma, (float2*)Wx, (float2*)dWx, (float*)w,
-                     idx, tb.status};
+                     idx, idx_pitch, tb.status};
     e = run_cwt_f32(op, B, m, (float2*)zb, zbytes / sizeof(float2), tb, st);
   } else if (precision == SSQB_F32X) {
     CwtOp<double2, float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,
                               1.0 / Npad, gamma, (float2*)Wx, (float2*)dWx, (float*)w,
-                              idx, tb.status};
+                              idx, idx_pitch, tb.status};
     e = run_cwt_f32x(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st);
   } else {
     CwtOp<double2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt, 1.0 / Npad,
-                      gamma, (double2*)Wx, (double2*)dWx, (double*)w, idx, tb.status};
+                      gamma, (double2*)Wx, (double2*)dWx, (double*)w, idx, idx_pitch,
+                      tb.status};
     e = run_cwt_f64(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st);
   }
   if (e) return cuda_fail((cudaError_t)e, "cwt launch");
   return SSQB_OK;
 }
 
-static int squeeze_common(const void* Wx, int kind, const void* src, const double* sfs,
-                          const double* cst, const ssqb_bins* bins, double gamma, int B,
-                          int na, int N, int nbins, int precision, void* Tx, void* stream) {
+static int squeeze_common(const void* Wx, int kind, const void* src, int idx_pitch,
+                          const double* sfs, const double* cst, const ssqb_bins* bins,
+                          double gamma, int B, int na, int N, int nbins, int precision,
+                          void* Tx, void* stream) {
   if (!Wx || !src || !cst || !Tx) return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
   if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
@@ -262,6 +267,8 @@ static int squeeze_common(const void* Wx, int kind, const void* src, const doubl
     return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
   precision = data_prec(precision);
   if (nbins < 1 || nbins > 65535) return fail(SSQB_EINVAL, "nbins must be in [1, 65535]");
+  if (idx_pitch == 0) idx_pitch = N;
+  if (kind == 0 && idx_pitch < N) return fail(SSQB_EINVAL, "idx_pitch smaller than N");
   BinDev bd{};
   if (kind != 0) {
     int r = check_bins(bins, nbins, &bd);
@@ -277,39 +284,40 @@ static int squeeze_common(const void* Wx, int kind, const void* src, const doubl
   cudaStream_t st = (cudaStream_t)stream;
   int e;
   if (precision == SSQB_F32)
-    e = run_squeeze_f32((const float2*)Wx, kind, src, sfs, bd, gamma, cst, B, na, N, nbins,
-                        (float2*)Tx, tb.status, st);
+    e = run_squeeze_f32((const float2*)Wx, kind, src, idx_pitch, sfs, bd, gamma, cst, B, na,
+                        N, nbins, (float2*)Tx, tb.status, st);
   else
-    e = run_squeeze_f64((const double2*)Wx, kind, src, sfs, bd, gamma, cst, B, na, N, nbins,
-                        (double2*)Tx, tb.status, st);
+    e = run_squeeze_f64((const double2*)Wx, kind, src, idx_pitch, sfs, bd, gamma, cst, B, na,
+                        N, nbins, (double2*)Tx, tb.status, st);
   if (e) return cuda_fail((cudaError_t)e, "squeeze launch");
   return SSQB_OK;
 }
 
-int ssqb_squeeze(const void* Wx, const uint16_t* idx, const double* row_weights, int B,
-                 int na, int N, int nbins, int precision, void* Tx, void* stream) {
-  return squeeze_common(Wx, 0, idx, nullptr, row_weights, nullptr, 0.0, B, na, N, nbins,
-                        precision, Tx, stream);
+int ssqb_squeeze(const void* Wx, const uint16_t* idx, int idx_pitch,
+                 const double* row_weights, int B, int na, int N, int nbins, int precision,
+                 void* Tx, void* stream) {
+  return squeeze_common(Wx, 0, idx, idx_pitch, nullptr, row_weights, nullptr, 0.0, B, na, N,
+                        nbins, precision, Tx, stream);
 }
 
 int ssqb_ssqueeze_fast(const void* Wx, const void* dWx, const double* Sfs,
                        const double* row_weights, const ssqb_bins* bins, double gamma,
                        int B, int na, int N, int precision, void* Tx, void* stream) {
-  return squeeze_common(Wx, 1, dWx, Sfs, row_weights, bins, gamma, B, na, N,
+  return squeeze_common(Wx, 1, dWx, 0, Sfs, row_weights, bins, gamma, B, na, N,
                         bins ? bins->nbins : 0, precision, Tx, stream);
 }
 
 int ssqb_indexed_sum(const void* Wx, const void* w, const double* row_weights,
                      const ssqb_bins* bins, int B, int na, int N, int precision, void* Tx,
                      void* stream) {
-  return squeeze_common(Wx, 2, w, nullptr, row_weights, bins, 0.0, B, na, N,
+  return squeeze_common(Wx, 2, w, 0, nullptr, row_weights, bins, 0.0, B, na, N,
                         bins ? bins->nbins : 0, precision, Tx, stream);
 }
 
 int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padtype,
               int modulated, const double* window, const double* diff_window,
               const double* Sfs, const ssqb_bins* bins, double gamma, int precision,
-              void* Sx, void* dSx, void* w, uint16_t* idx, void* stream) {
+              void* Sx, void* dSx, void* w, uint16_t* idx, int idx_pitch, void* stream) {
   if (!x || !window || !diff_window || !Sfs || !Sx)
     return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || hop < 1) return fail(SSQB_EINVAL, "B, N and hop must be >= 1");
@@ -320,6 +328,9 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
   if (!valid_precision(precision))
     return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
   const int nrow = n_fft / 2 + 1;
+  const int nframes = (N - 1) / hop + 1;
+  if (idx_pitch == 0) idx_pitch = nframes;
+  if (idx && idx_pitch < nframes) return fail(SSQB_EINVAL, "idx_pitch smaller than n_frames");
   BinDev bd{};
   if (idx) {
     int r = check_bins(bins, nrow, &bd);
@@ -329,7 +340,6 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
   int r = get_tables(&tb);
   if (r) return r;
   cudaStream_t st = (cudaStream_t)stream;
-  const int nframes = (N - 1) / hop + 1;
   const int s20 = (n_fft + 1) / 2;
   const int s21 = (n_fft % 2 == 1) ? s20 - 1 : s20;
   const int m = ilog2i(n_fft);
@@ -337,18 +347,19 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
   if (precision == SSQB_F32) {
     StftOp<float, float2> op{(const float*)x, window, diff_window, Sfs, bd, N, n_fft, hop,
                              n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
-                             (float2*)Sx, (float2*)dSx, (float*)w, idx, tb.status};
+                             (float2*)Sx, (float2*)dSx, (float*)w, idx, idx_pitch, tb.status};
     e = run_stft_f32(op, B, m, tb, st);
   } else if (precision == SSQB_F32X) {
     StftOp<float, double2, float2> op{(const float*)x, window, diff_window, Sfs, bd, N,
                                       n_fft, hop, n1, padtype, s21, modulated ? 1 : 0,
                                       nframes, gamma, (float2*)Sx, (float2*)dSx, (float*)w,
-                                      idx, tb.status};
+                                      idx, idx_pitch, tb.status};
     e = run_stft_f32x(op, B, m, tb, st);
   } else {
     StftOp<double, double2> op{(const double*)x, window, diff_window, Sfs, bd, N, n_fft,
                                hop, n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
-                               (double2*)Sx, (double2*)dSx, (double*)w, idx, tb.status};
+                               (double2*)Sx, (double2*)dSx, (double*)w, idx, idx_pitch,
+                               tb.status};
     e = run_stft_f64(op, B, m, tb, st);
   }
   if (e) return cuda_fail((cudaError_t)e, "stft launch");

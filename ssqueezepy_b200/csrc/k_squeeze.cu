@@ -1,6 +1,7 @@
 // Squeeze kernel instantiations and launchers.
 #include "launch.h"
 #include "squeeze.cuh"
+#include "squeeze_bulk.cuh"
 
 namespace ssqb {
 
@@ -18,14 +19,34 @@ static int launch_sq(const C* Wx, const Src& src, const double* cst, int B, int 
   return cudaGetLastError();
 }
 
+static int launch_sq_bulk(const float2* Wx, const uint16_t* idx, int pitch,
+                          const double* cst, int B, int na, int N, int nbins, float2* Tx,
+                          int* status, cudaStream_t st) {
+  const size_t smem = sizeof(SqRing) + (size_t)nbins * 32 * sizeof(float2) +
+                      (size_t)na * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(squeeze_bulk_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e) return e;
+  dim3 grid((N + 31) / 32, B);
+  squeeze_bulk_kernel<<<grid, 32, smem, st>>>(Wx, idx, pitch, cst, na, N, nbins, Tx, status);
+  return cudaGetLastError();
+}
+
 template <typename C>
-static int run_sq(const C* Wx, int src_kind, const void* src, const double* sfs,
-                  const BinDev& bins, double gamma, const double* cst, int B, int na, int N,
-                  int nbins, C* Tx, int* status, cudaStream_t st) {
+static int run_sq(const C* Wx, int src_kind, const void* src, int idx_pitch,
+                  const double* sfs, const BinDev& bins, double gamma, const double* cst,
+                  int B, int na, int N, int nbins, C* Tx, int* status, cudaStream_t st) {
   typedef typename RealOf<C>::type T;
   switch (src_kind) {
     case 0: {
-      IdxSrc<C> s{(const uint16_t*)src};
+      if constexpr (sizeof(C) == 8) {
+        const size_t smem = sizeof(SqRing) + (size_t)nbins * 32 * sizeof(float2) +
+                            (size_t)na * sizeof(float);
+        if (N % 2 == 0 && idx_pitch % 32 == 0 && smem <= 227 * 1024)
+          return launch_sq_bulk((const float2*)Wx, (const uint16_t*)src, idx_pitch, cst, B,
+                                na, N, nbins, (float2*)Tx, status, st);
+      }
+      IdxSrc<C> s{(const uint16_t*)src, idx_pitch, N};
       return launch_sq(Wx, s, cst, B, na, N, nbins, Tx, status, st);
     }
     case 1: {
@@ -41,18 +62,20 @@ static int run_sq(const C* Wx, int src_kind, const void* src, const double* sfs,
   }
 }
 
-int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, const double* sfs,
-                    const BinDev& bins, double gamma, const double* cst, int B, int na,
-                    int N, int nbins, float2* Tx, int* status, cudaStream_t st) {
-  return run_sq<float2>(Wx, src_kind, src, sfs, bins, gamma, cst, B, na, N, nbins, Tx,
-                        status, st);
+int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, int idx_pitch,
+                    const double* sfs, const BinDev& bins, double gamma, const double* cst,
+                    int B, int na, int N, int nbins, float2* Tx, int* status,
+                    cudaStream_t st) {
+  return run_sq<float2>(Wx, src_kind, src, idx_pitch, sfs, bins, gamma, cst, B, na, N,
+                        nbins, Tx, status, st);
 }
 
-int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, const double* sfs,
-                    const BinDev& bins, double gamma, const double* cst, int B, int na,
-                    int N, int nbins, double2* Tx, int* status, cudaStream_t st) {
-  return run_sq<double2>(Wx, src_kind, src, sfs, bins, gamma, cst, B, na, N, nbins, Tx,
-                         status, st);
+int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, int idx_pitch,
+                    const double* sfs, const BinDev& bins, double gamma, const double* cst,
+                    int B, int na, int N, int nbins, double2* Tx, int* status,
+                    cudaStream_t st) {
+  return run_sq<double2>(Wx, src_kind, src, idx_pitch, sfs, bins, gamma, cst, B, na, N,
+                         nbins, Tx, status, st);
 }
 
 }  // namespace ssqb

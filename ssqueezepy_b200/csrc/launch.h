@@ -42,13 +42,16 @@ int run_stft_f64(const StftOp<double, double2>& op, int B, int log2L,
 int run_stft_f32x(const StftOp<float, double2, float2>& op, int B, int log2L,
                   const Tables& tb, cudaStream_t st);
 
-// squeeze; src_kind 0 = uint16 index, 1 = phase from dWx (cwt or stft), 2 = w
-int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, const double* sfs,
-                    const BinDev& bins, double gamma, const double* cst, int B, int na,
-                    int N, int nbins, float2* Tx, int* status, cudaStream_t st);
-int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, const double* sfs,
-                    const BinDev& bins, double gamma, const double* cst, int B, int na,
-                    int N, int nbins, double2* Tx, int* status, cudaStream_t st);
+// squeeze; src_kind 0 = uint16 index (rows of idx_pitch), 1 = phase from dWx
+// (cwt or stft), 2 = w
+int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, int idx_pitch,
+                    const double* sfs, const BinDev& bins, double gamma, const double* cst,
+                    int B, int na, int N, int nbins, float2* Tx, int* status,
+                    cudaStream_t st);
+int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, int idx_pitch,
+                    const double* sfs, const BinDev& bins, double gamma, const double* cst,
+                    int B, int na, int N, int nbins, double2* Tx, int* status,
+                    cudaStream_t st);
 
 int run_icwt(const void* Wx, const double* w, const double* x_mean, double mean_weight,
              int B, int na, int N, int precision, void* x, cudaStream_t st);

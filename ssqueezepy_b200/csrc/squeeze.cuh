@@ -15,8 +15,11 @@ namespace ssqb {
 template <typename C>
 struct IdxSrc {
   const uint16_t* idx;
+  int pitch, N;  // idx rows of `pitch` columns; Wx rows of N
   struct Pre { uint16_t k; };
-  __device__ __forceinline__ Pre pre(size_t o) const { return Pre{__ldg(idx + o)}; }
+  __device__ __forceinline__ Pre pre(size_t o) const {
+    return Pre{__ldg(idx + (o / N) * pitch + o % N)};
+  }
   __device__ __forceinline__ int bin(const Pre& p, C, int) const {
     return p.k == kNoBin ? -1 : (int)p.k;
   }

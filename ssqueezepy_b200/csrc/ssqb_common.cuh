@@ -68,6 +68,7 @@ enum DeviceStatus : int {
   DEV_OK = 0,
   DEV_BAD_BIN = 1,      // a bin index fell outside [0, nbins)
   DEV_BAD_INDEX = 2,    // a padded-signal index fell outside the signal
+  DEV_TIMEOUT = 3,      // a bounded wait on an asynchronous copy expired
 };
 
 __device__ __forceinline__ void set_status(int* st, int code) {

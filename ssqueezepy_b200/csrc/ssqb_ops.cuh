@@ -178,7 +178,8 @@ struct CwtOp {
   OC* Wx;                 // (B, na, N)
   OC* dWx;                // optional
   OT* w;                  // optional phase transform
-  uint16_t* idx;          // optional bin index
+  uint16_t* idx;          // optional bin index, (B, na, idx_pitch)
+  int idx_pitch;
   int* status;
   __device__ int rows() const { return na; }
   __device__ void load(int b, int row, int k, C (&v)[2]) const {
@@ -206,7 +207,7 @@ struct CwtOp {
       double wv;
       const uint16_t k = phase_bin(Wv, dWv, 0.0, false, bins, gamma, status,
                                    w ? &wv : nullptr);
-      if (idx) idx[o] = k;
+      if (idx) idx[((size_t)b * na + row) * idx_pitch + j] = k;
       if (w) w[o] = (OT)wv;
     }
   }
@@ -229,7 +230,8 @@ struct StftOp {
   OC* Sx;                  // (B, L/2+1, nframes)
   OC* dSx;
   OT* w;
-  uint16_t* idx;
+  uint16_t* idx;           // (B, L/2+1, idx_pitch)
+  int idx_pitch;
   int* status;
   __device__ int rows() const { return nframes; }
   __device__ void load(int b, int t, int m, C (&v)[1]) const {
@@ -257,7 +259,7 @@ struct StftOp {
       double wv;
       const uint16_t k = phase_bin(S, dS, __ldg(sfs + n), true, bins, gamma, status,
                                    w ? &wv : nullptr);
-      if (idx) idx[o] = k;
+      if (idx) idx[((size_t)b * nrow + n) * idx_pitch + t] = k;
       if (w) w[o] = (OT)wv;
     }
   }

@@ -35,12 +35,12 @@ def _cwt_call(**kw):
     a = dict(x=ctypes.c_void_p(8), B=1, N=100, Npad=256, n1=78, padtype=1, rpadded=0,
              scales=ctypes.c_void_p(8), na=10, wav=L.make_wavelet(0, (6., 1e-8, 1., 0.)),
              dt=1.0, bins=None, gamma=1e-6, prec=0, Wx=ctypes.c_void_p(8), dWx=None,
-             w=None, idx=None, ws=ctypes.c_void_p(8), wsb=1 << 30, st=None)
+             w=None, idx=None, ipitch=0, ws=ctypes.c_void_p(8), wsb=1 << 30, st=None)
     a.update(kw)
     return lib.ssqb_cwt(a['x'], a['B'], a['N'], a['Npad'], a['n1'], a['padtype'],
                         a['rpadded'], a['scales'], a['na'], a['wav'], a['dt'],
                         a['bins'], a['gamma'], a['prec'], a['Wx'], a['dWx'], a['w'],
-                        a['idx'], a['ws'], a['wsb'], a['st'])
+                        a['idx'], a['ipitch'], a['ws'], a['wsb'], a['st'])
 
 
 @pytest.mark.parametrize('kw, code', [
@@ -51,6 +51,8 @@ def _cwt_call(**kw):
     (dict(n1=200), L.EINVAL),
     (dict(padtype=9), L.EINVAL),
     (dict(prec=3), L.EINVAL),
+    (dict(idx=ctypes.c_void_p(8), ipitch=50,
+          bins=L.make_bins(0, (0., 0.1, 0, 0, 0), 10, 1)), L.EINVAL),
     (dict(dt=0.0), L.EINVAL),
     (dict(x=None), L.EINVAL),
     (dict(Wx=None), L.EINVAL),
@@ -68,16 +70,17 @@ def test_cwt_rejects_bad_arguments(kw, code):
 def test_other_entry_points_reject_bad_arguments():
     lib = L.load()
     p = ctypes.c_void_p(8)
-    assert lib.ssqb_squeeze(p, p, p, 0, 10, 10, 10, 0, p, None) == L.EINVAL
-    assert lib.ssqb_squeeze(p, p, p, 1, 10, 10, 70000, 0, p, None) == L.EINVAL
-    assert lib.ssqb_squeeze(p, p, p, 1, 10, 10, 10000, 0, p, None) == L.EUNSUPPORTED
+    assert lib.ssqb_squeeze(p, p, 0, p, 0, 10, 10, 10, 0, p, None) == L.EINVAL
+    assert lib.ssqb_squeeze(p, p, 0, p, 1, 10, 10, 70000, 0, p, None) == L.EINVAL
+    assert lib.ssqb_squeeze(p, p, 0, p, 1, 10, 10, 10000, 0, p, None) == L.EUNSUPPORTED
+    assert lib.ssqb_squeeze(p, p, 5, p, 1, 10, 10, 10, 0, p, None) == L.EINVAL
     assert lib.ssqb_ssqueeze_fast(p, p, None, p, None, 1e-6, 1, 5, 5, 0, p, None) \
         == L.EINVAL
     b = L.make_bins(2, (0., 0.1, 0, 0, 0), 65, 0)
     assert lib.ssqb_stft(p, 1, 100, 100, 1, 50, 1, 1, p, p, p, b, 1e-6, 0, p, None,
-                         None, None, None) == L.EUNSUPPORTED
+                         None, None, 0, None) == L.EUNSUPPORTED
     assert lib.ssqb_stft(p, 1, 100, 128, 0, 64, 1, 1, p, p, p, b, 1e-6, 0, p, None,
-                         None, None, None) == L.EINVAL
+                         None, None, 0, None) == L.EINVAL
     assert lib.ssqb_icwt(None, p, None, 1.0, 1, 10, 10, 0, p, None) == L.EINVAL
 
 

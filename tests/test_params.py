@@ -94,3 +94,17 @@ def test_bad_args():
         P.Wavelet(('gmw', {'gamma': -1}))
     with pytest.raises(Exception):
         P.process_fs_and_t(None, np.array([0, 1, 3.]), 3)
+
+
+def test_ssq_plan_weights_follow_scale_array():
+    """log-piecewise scales: the squeeze weight is ln2/nv per row, nv read
+    from the scale array (32 below the transition, 8 above), as ssqueeze
+    re-derives it (ssqueezing.py:168-169, 124-128)."""
+    from ssqueezepy_b200 import _transforms as T
+    w = P.Wavelet(('morlet', {'mu': 6.}))
+    fp = T._ssq_plan(w, 'log-piecewise', 10000, 32, 'log', 'peak', 'reflect', 1.)
+    c = fp['const']
+    s = P.process_scales('log-piecewise', 10000, w, nv=32).ravel()
+    idx = P.logscale_transition_idx(s)
+    assert idx is not None
+    assert np.allclose(c[:idx], np.log(2) / 32) and np.allclose(c[idx:], np.log(2) / 8)
