@@ -93,6 +93,9 @@ static int check_wavelet(const ssqb_wavelet* w, WavDev* out) {
   out->wcg = (w->kind == 1) ? std::pow(w->p[2], w->p[0]) : 0.0;
   out->lo = w->band[0];
   out->hi = w->band[1];
+  out->ibeta = -1;
+  if (w->kind == 1 && w->p[1] >= 0 && w->p[1] <= 128 && w->p[1] == std::floor(w->p[1]))
+    out->ibeta = (int)w->p[1];
   if (w->kind != 0 && !(w->p[0] > 0 && w->p[1] > 0))
     return fail(SSQB_EINVAL, "GMW gamma and beta must be positive");
   return SSQB_OK;
@@ -274,8 +277,8 @@ static int squeeze_common(const void* Wx, int kind, const void* src, int idx_pit
     int r = check_bins(bins, nbins, &bd);
     if (r) return r;
   }
-  const size_t smem = (size_t)nbins * 32 * csize(precision) +
-                      (size_t)na * (precision == SSQB_F64 ? 8 : 4);  // data precision
+  const size_t smem = (size_t)nbins * 8 * csize(precision) +
+                      (size_t)na * (precision == SSQB_F64 ? 8 : 4);  // 8 columns per warp
   if (smem > 227 * 1024)
     return fail(SSQB_EUNSUPPORTED, "too many bins for the shared-memory squeeze");
   Tables tb;

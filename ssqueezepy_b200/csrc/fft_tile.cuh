@@ -147,7 +147,9 @@ template <> __device__ __forceinline__ const double2* seg_table<double2>(const T
 
 // One full transform of the tile.
 //   ld(f, m, C (&v)[NARR])   input element m of row f (all arrays)
-//   st(f, m, C (&v)[NARR])   output element m of row f (when DIRECT_OUT)
+//   st.item<R>(f, m0, stride, C (&a)[R], C (&b)[R])
+//                            outputs m0 + r*stride of row f, r < R, of the
+//                            first and last array (when DIRECT_OUT)
 // buf: NARR arrays of Layout::ARR elements. MAP_IN / MAP_OUT: mappings of the
 // first and last stage; middle stages use MAP_J. With DIRECT_OUT == false the
 // last stage writes shared memory (read it back with Layout::at after the
@@ -213,17 +215,14 @@ __device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __rest
 #pragma unroll
       for (int a = 0; a < NARR; ++a) dft<R, SIGN>(v[a][p]);
       const int base = ((j >> LNS) << (LNS + RL)) + k;
+      if constexpr (LAST && DIRECT_OUT) {
+        // outputs base + r*NS of row f, r = 0..R-1, handed over together
+        st.template item<R>(f, base, NS, v[0][p], v[NARR - 1][p]);
+      } else {
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if constexpr (LAST && DIRECT_OUT) {
-          C t[NARR];
-#pragma unroll
-          for (int a = 0; a < NARR; ++a) t[a] = v[a][p][r];
-          st(f, base + r * NS, t);
-        } else {
+        for (int r = 0; r < R; ++r)
 #pragma unroll
           for (int a = 0; a < NARR; ++a) buf[a][LY::at(f, base + r * NS)] = v[a][p][r];
-        }
       }
     }
   }

@@ -1,34 +1,30 @@
 // Squeeze kernel instantiations and launchers.
 #include "launch.h"
 #include "squeeze.cuh"
-#include "squeeze_bulk.cuh"
 
 namespace ssqb {
+
+// Lane layout G (rows per warp instruction): the accumulator of a warp is
+// nbins x 32/G; G = 4 keeps it small enough for about ten warps per SM.
+#ifndef SSQB_SQ_G
+#define SSQB_SQ_G 4
+#endif
+#ifndef SSQB_SQ_U
+#define SSQB_SQ_U 8
+#endif
 
 template <typename C, class Src>
 static int launch_sq(const C* Wx, const Src& src, const double* cst, int B, int na, int N,
                      int nbins, C* Tx, int* status, cudaStream_t st) {
   typedef typename RealOf<C>::type T;
-  const size_t smem = (size_t)nbins * 32 * sizeof(C) + (size_t)na * sizeof(T);
-  auto k = squeeze_kernel<C, Src>;
+  constexpr int G = SSQB_SQ_G, U = SSQB_SQ_U, CW = 32 / G;
+  const size_t smem = (size_t)nbins * CW * sizeof(C) + (size_t)na * sizeof(T);
+  auto k = squeeze_kernel<C, Src, G, U>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e) return e;
-  dim3 grid((N + 31) / 32, B);
+  dim3 grid((N + CW - 1) / CW, B);
   k<<<grid, 32, smem, st>>>(Wx, src, cst, na, N, nbins, Tx, status);
-  return cudaGetLastError();
-}
-
-static int launch_sq_bulk(const float2* Wx, const uint16_t* idx, int pitch,
-                          const double* cst, int B, int na, int N, int nbins, float2* Tx,
-                          int* status, cudaStream_t st) {
-  const size_t smem = sizeof(SqRing) + (size_t)nbins * 32 * sizeof(float2) +
-                      (size_t)na * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(squeeze_bulk_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e) return e;
-  dim3 grid((N + 31) / 32, B);
-  squeeze_bulk_kernel<<<grid, 32, smem, st>>>(Wx, idx, pitch, cst, na, N, nbins, Tx, status);
   return cudaGetLastError();
 }
 
@@ -39,13 +35,6 @@ static int run_sq(const C* Wx, int src_kind, const void* src, int idx_pitch,
   typedef typename RealOf<C>::type T;
   switch (src_kind) {
     case 0: {
-      if constexpr (sizeof(C) == 8) {
-        const size_t smem = sizeof(SqRing) + (size_t)nbins * 32 * sizeof(float2) +
-                            (size_t)na * sizeof(float);
-        if (N % 2 == 0 && idx_pitch % 32 == 0 && smem <= 227 * 1024)
-          return launch_sq_bulk((const float2*)Wx, (const uint16_t*)src, idx_pitch, cst, B,
-                                na, N, nbins, (float2*)Tx, status, st);
-      }
       IdxSrc<C> s{(const uint16_t*)src, idx_pitch, N};
       return launch_sq(Wx, s, cst, B, na, N, nbins, Tx, status, st);
     }

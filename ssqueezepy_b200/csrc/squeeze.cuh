@@ -1,11 +1,10 @@
 // Deterministic synchrosqueeze: Tx[k(i,j), j] += Wx[i,j] * c_i.
 //
-// One warp owns 32 consecutive time columns of one signal and keeps their
-// whole Tx column block, nbins x 32, in shared memory. Lane l walks the rows
-// i = 0..na-1 of column j0+l in ascending order, the order of the reference's
-// per-column loop (algos.py:879-895), so every bin accumulates in a fixed
-// order: no atomics, results independent of scheduling. Loads of Wx and of
-// the bin source are issued U rows ahead of the shared-memory updates.
+// One warp owns a few consecutive time columns of one signal and keeps their
+// whole Tx column block, nbins x columns, in shared memory. Each bin of a
+// column receives its rows in ascending order, the order of the reference's
+// per-column loop (algos.py:879-895): no atomics, results independent of
+// scheduling.
 #pragma once
 #include "ssqb_ops.cuh"
 
@@ -60,64 +59,69 @@ struct WSrc {
   }
 };
 
-constexpr int kSqU = 8;  // rows in flight per lane
-
-template <typename C, class Src>
+// Lane layout: a warp covers G rows x CW = 32/G columns; lane = g*CW + c
+// handles column j0 + c of rows i = i0 + g, i0 + G + g, ... The G lanes of a
+// column update the shared accumulator in G ordered phases (__syncwarp
+// between them), so every bin still receives its rows in ascending order.
+// Loads for U row groups are issued before their updates.
+template <typename C, class Src, int G, int U>
 __global__ void __launch_bounds__(32)
 squeeze_kernel(const C* __restrict__ Wx, Src src, const double* __restrict__ cst,
                int na, int N, int nbins, C* __restrict__ Tx, int* status) {
   typedef typename RealOf<C>::type T;
+  constexpr int CW = 32 / G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* acc = reinterpret_cast<C*>(smem_raw);           // [nbins][32]
-  T* cs = reinterpret_cast<T*>(acc + (size_t)nbins * 32);  // [na]
+  C* acc = reinterpret_cast<C*>(smem_raw);                   // [nbins][CW]
+  T* cs = reinterpret_cast<T*>(acc + (size_t)nbins * CW);   // [na]
   const int lane = threadIdx.x;
+  const int g = lane / CW, c = lane % CW;
   const int b = blockIdx.y;
-  const int j = blockIdx.x * 32 + lane;
+  const int j = blockIdx.x * CW + c;
   const bool live = j < N;
-  for (int k = lane; k < nbins * 32; k += 32) acc[k] = mk((T)0, (T)0);
+  for (int k = lane; k < nbins * CW; k += 32) acc[k] = mk((T)0, (T)0);
   for (int i = lane; i < na; i += 32) cs[i] = (T)cst[i];
   __syncwarp();
   const size_t base = (size_t)b * na * N + j;
-  int i = 0;
-  for (; i + kSqU <= na; i += kSqU) {
-    C v[kSqU];
-    typename Src::Pre p[kSqU];
+  for (int i0 = 0; i0 < na; i0 += G * U) {
+    C v[U];
+    typename Src::Pre p[U];
+    bool ok[U];
 #pragma unroll
-    for (int u = 0; u < kSqU; ++u) {
-      const size_t o = base + (size_t)(i + u) * N;
-      if (live) { v[u] = Wx[o]; p[u] = src.pre(o); }
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * G + g;
+      ok[u] = live && i < na;
+      if (ok[u]) {
+        const size_t o = base + (size_t)i * N;
+        v[u] = Wx[o];
+        p[u] = src.pre(o);
+      }
     }
 #pragma unroll
-    for (int u = 0; u < kSqU; ++u) {
-      if (!live) continue;
-      const int k = src.bin(p[u], v[u], i + u);
-      if (k >= nbins) { set_status(status, DEV_BAD_BIN); continue; }
-      if (k >= 0) {
-        C& a = acc[k * 32 + lane];
-        const T c = cs[i + u];
-        a.x += v[u].x * c;
-        a.y += v[u].y * c;
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * G + g;
+      int k = -1;
+      if (ok[u]) {
+        k = src.bin(p[u], v[u], i);
+        if (k >= nbins) { set_status(status, DEV_BAD_BIN); k = -1; }
+      }
+#pragma unroll
+      for (int ph = 0; ph < G; ++ph) {
+        if (ph == g && k >= 0) {
+          C& a = acc[k * CW + c];
+          const T w = cs[i];
+          a.x += v[u].x * w;
+          a.y += v[u].y * w;
+        }
+        if (G > 1) __syncwarp();
       }
     }
   }
-  for (; i < na; ++i) {
-    if (!live) break;
-    const size_t o = base + (size_t)i * N;
-    const C v = Wx[o];
-    const typename Src::Pre p = src.pre(o);
-    const int k = src.bin(p, v, i);
-    if (k >= nbins) { set_status(status, DEV_BAD_BIN); continue; }
-    if (k >= 0) {
-      C& a = acc[k * 32 + lane];
-      const T c = cs[i];
-      a.x += v.x * c;
-      a.y += v.y * c;
-    }
-  }
   __syncwarp();
-  if (live) {
-    C* out = Tx + (size_t)b * nbins * N + j;
-    for (int k = 0; k < nbins; ++k) out[(size_t)k * N] = acc[k * 32 + lane];
+  C* out = Tx + (size_t)b * nbins * N + blockIdx.x * CW;
+  const int ncol = min(CW, N - (int)blockIdx.x * CW);
+  for (int e = lane; e < nbins * CW; e += 32) {
+    const int k = e / CW, cc = e % CW;
+    if (cc < ncol) out[(size_t)k * N + cc] = acc[e];
   }
 }
 

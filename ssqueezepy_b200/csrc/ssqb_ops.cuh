@@ -12,7 +12,19 @@ struct WavDev {
   double p0, p1, p2, p3;  // Morlet: mu, ks, C1; GMW: gamma, beta, wc, wcl | l2norm
   double wcg;        // GMW: wc^gamma
   double lo, hi;     // psih = 0 outside [lo, hi] (skipped when lo >= hi)
+  int ibeta;         // GMW L1: beta when it is an integer in [0, 128], else -1
 };
+
+// x^n for 0 <= n < 256 by binary powering (relative error ~ a few ulps)
+__device__ __forceinline__ double powi(double x, int n) {
+  double r = 1.0, p = x;
+#pragma unroll
+  for (int bit = 0; bit < 8; ++bit) {
+    if (n & (1 << bit)) r *= p;
+    p *= p;
+  }
+  return r;
+}
 
 struct BinDev {
   int mode;          // 0 log, 1 log-piecewise, 2 linear
@@ -70,6 +82,11 @@ __device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
     return w.p2 * (ea - w.p1 * ec);
   }
   if (x <= 0.0) return 0.0;
+  if (w.kind == 1 && w.ibeta >= 0 && w.p0 == 3.0) {
+    // 2 exp(beta ln(x/wc) - (x^3 - wc^3)) = 2 (x/wc)^beta exp(wc^3 - x^3)
+    const double e = w.wcg - x * x * x;
+    return e > -708.0 ? 2.0 * powi(x / w.p2, w.ibeta) * exp(e) : 0.0;
+  }
   const double lw = log(x);
   const double xg = (w.p0 == 3.0) ? x * x * x : exp(w.p0 * lw);
   if (w.kind == 1) {
@@ -102,21 +119,73 @@ __device__ __forceinline__ int bin_of(const BinDev& bp, double w) {
   return ki;
 }
 
-// Phase transform and bin of one (Wx, dWx) pair, float64 from the stored
-// values (algos.py:864-876): w = |Im(dWx conj Wx)| / (|Wx|^2 2pi), Sfs shift
-// for the STFT (algos.py:963-964). Returns kNoBin where |Wx| <= gamma.
+// Bin position in float32 with a guard band: returns the bin, or -2 when
+// the position lies within kBinGuard of a rounding edge (or of the
+// log-piecewise split), where only the float64 decision is trusted. The
+// float32 position carries ~1e-5 bins of error at most here (phase transform
+// ~1e-7 relative -> ~5e-6 bins; log2f and the float32 affine map ~2e-5).
+constexpr float kBinGuard = 2.5e-4f;
+__device__ __forceinline__ int bin_of_fast(const BinDev& bp, float w) {
+  const float omax = (float)(bp.nbins - 1);
+  float pos, lo_clamp = 0.f;
+  int add = 0;
+  if (bp.mode == 2) {
+    pos = (w - (float)bp.p0) * (float)(1.0 / bp.p1);
+  } else {
+    const float wl = log2f(w);
+    if (bp.mode == 0) {
+      pos = (wl - (float)bp.p0) * (float)(1.0 / bp.p1);
+    } else {
+      const float split = (float)bp.p1;  // vlmin1
+      if (fabsf(wl - split) < 1e-4f * fmaxf(1.f, fabsf(split))) return -2;
+      if (wl > split) {
+        pos = (wl - split) * (float)(1.0 / bp.p3);
+        add = bp.idx1;
+        lo_clamp = -3.0e38f;
+      } else {
+        pos = (wl - (float)bp.p0) * (float)(1.0 / bp.p2);
+      }
+    }
+  }
+  const float fr = pos - floorf(pos);
+  if (!(fabsf(fr - 0.5f) >= kBinGuard)) return -2;  // also catches NaN
+  const float k = fminf(fmaxf(rintf(pos), lo_clamp) + (float)add, omax);
+  int ki = (int)fmaxf(k, 0.f);
+  if (bp.mode == 1 && add == 0) ki = (int)fmaxf(rintf(pos), 0.f);
+  if (bp.flipud) ki = bp.nbins - 1 - ki;
+  return ki;
+}
+
+// Phase transform and bin of one (Wx, dWx) pair (algos.py:864-876): w =
+// |Im(dWx conj Wx)| / (|Wx|^2 2pi), Sfs shift for the STFT (algos.py:963-964).
+// The bin is decided in float32 when that is safe, else in float64; either
+// way it equals the float64 decision from these values. Returns kNoBin where
+// |Wx| <= gamma.
 template <typename C>
 __device__ __forceinline__ uint16_t phase_bin(C Wv, C dWv, double sfs, bool stft,
                                               const BinDev& bp, double gamma,
                                               int* status, double* w_out) {
   const double c = Wv.x, d = Wv.y, a = dWv.x, b = dWv.y;
   const double m2 = c * c + d * d;
-  const double mag = sqrt(m2);
-  const double ph = (b * c - a * d) / (m2 * kTwoPi);
-  const double w = stft ? fabs(sfs - ph) : fabs(ph);
-  if (w_out) *w_out = (mag < gamma) ? __longlong_as_double(0x7ff0000000000000ULL) : w;
-  if (!(mag > gamma)) return kNoBin;
-  const int k = bin_of(bp, w);
+  const double num = b * c - a * d;
+  const bool keep = m2 > gamma * gamma;  // |Wx| > gamma
+  if (w_out) {
+    const double ph = num / (m2 * kTwoPi);
+    const double wv = stft ? fabs(sfs - ph) : fabs(ph);
+    *w_out = (m2 < gamma * gamma) ? __longlong_as_double(0x7ff0000000000000ULL) : wv;
+  }
+  if (!keep) return kNoBin;
+  int k = -2;
+  {
+    const float ph32 = (float)num / ((float)m2 * 6.2831855f);
+    const float w32 = stft ? fabsf((float)sfs - ph32) : fabsf(ph32);
+    if (w32 > 0.f && w32 < 3.0e38f) k = bin_of_fast(bp, w32);
+  }
+  if (k == -2) {
+    const double ph = num / (m2 * kTwoPi);
+    const double w = stft ? fabs(sfs - ph) : fabs(ph);
+    k = bin_of(bp, w);
+  }
   if (k < 0 || k >= bp.nbins || k >= (int)kNoBin) {
     set_status(status, DEV_BAD_BIN);
     return kNoBin;

@@ -28,8 +28,64 @@ template <typename C> __host__ __device__ constexpr int tile_of() {
   return FftCfg<C>::TILE;
 }
 
+// CTAs per SM requested from the compiler (register budget per thread)
+#ifndef SSQB_FP64_MINBLOCKS
+#define SSQB_FP64_MINBLOCKS 2
+#endif
+template <typename C> struct MinBlocks { static constexpr int v = 2; };
+template <> struct MinBlocks<double2> { static constexpr int v = SSQB_FP64_MINBLOCKS; };
+
+// Storer handing each output to op.store. Single pass: row = row0 + f,
+// index m; pass 2: row fixed, index L2*m + n2_0 + f (mul = L2, add = n2_0).
+template <class Op, typename C>
+struct StoreEach {
+  static constexpr int NARR = Op::NARR;
+  const Op& op;
+  int b, row0, nrows, mul, add;
+  template <int R>
+  __device__ __forceinline__ void item(int f, int m0, int stride, C (&a)[R], C (&z)[R]) const {
+    const bool single = (nrows != 0x7fffffff);
+    const int row = single ? row0 + f : row0;
+    if (single && row >= nrows) return;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      C v[NARR];
+      v[0] = a[r];
+      v[NARR - 1] = z[r];
+      const int m = m0 + r * stride;
+      op.store(b, row, single ? m : mul * m + add + f, v);
+    }
+  }
+};
+
+// Pass-1 storer: Z[a][n2][k1] = v * w_L^(k1*n2) for n2 = m0 + r*stride, the
+// twiddles by recurrence from two table values (float64).
+template <typename C, int NARR, int SIGN>
+struct Pass1Store {
+  const Tables& tb;
+  C* zrow;
+  int k1_0, L1, log2L;
+  template <int R>
+  __device__ __forceinline__ void item(int f, int m0, int stride, C (&a)[R], C (&z)[R]) const {
+    const int k1 = k1_0 + f;
+    const uint64_t mask = ((uint64_t)1 << log2L) - 1;
+    const size_t L = (size_t)1 << log2L;
+    double2 w = unit_root<SIGN>(tb, (uint32_t)(((uint64_t)k1 * (uint64_t)m0) & mask), log2L);
+    const double2 s =
+        unit_root<SIGN>(tb, (uint32_t)(((uint64_t)k1 * (uint64_t)stride) & mask), log2L);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const C wc = to_c<C>(w);
+      const size_t o = size_t(m0 + r * stride) * L1 + k1;
+      zrow[o] = cmul(a[r], wc);
+      if constexpr (NARR > 1) zrow[L + o] = cmul(z[r], wc);
+      w = mk(w.x * s.x - w.y * s.y, w.x * s.y + w.y * s.x);
+    }
+  }
+};
+
 template <class Op, typename C, int LOGL, int SIGN>
-__global__ void __launch_bounds__(kNT)
+__global__ void __launch_bounds__(kNT, MinBlocks<C>::v)
 tile_single(Op op, Tables tb) {
   constexpr int NARR = Op::NARR;
   constexpr int TILE = tile_of<C>();
@@ -55,12 +111,10 @@ tile_single(Op op, Tables tb) {
     }
   };
   if constexpr (Op::kDirect) {
-    auto st = [&](int f, int m, C (&v)[NARR]) {
-      if (row0 + f < nrows) op.store(b, row0 + f, m, v);
-    };
+    StoreEach<Op, C> st{op, b, row0, nrows, 1, 0};
     fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, true>(buf, seg_table<C>(tb), ld, st);
   } else {
-    auto st = [&](int, int, C (&)[NARR]) {};
+    StoreEach<Op, C> st{op, b, row0, nrows, 1, 0};
     fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, false>(buf, seg_table<C>(tb), ld, st);
     for (int e = threadIdx.x; e < TILE; e += kNT) {
       const int f = e % NF, n = e / NF;  // rows fastest: coalesced (row, n) outputs
@@ -72,7 +126,7 @@ tile_single(Op op, Tables tb) {
 // pass 1: CTA = (k1 block of NF = TILE/L2 columns, row within the row tile,
 // batch item). Z layout: [b][row - row_lo][a][n2][k1].
 template <class Op, typename C, int LOGL2, int SIGN>
-__global__ void __launch_bounds__(kNT)
+__global__ void __launch_bounds__(kNT, MinBlocks<C>::v)
 tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_in_tile) {
   constexpr int NARR = Op::NARR;
   constexpr int TILE = tile_of<C>();
@@ -92,19 +146,13 @@ tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_
   const size_t L = size_t(1) << log2L;
   C* zrow = Z + (size_t(b) * rows_in_tile + blockIdx.y) * NARR * L;
   auto ld = [&](int f, int m, C (&v)[NARR]) { op.load(b, row, k1_0 + f + L1 * m, v); };
-  auto st = [&](int f, int m, C (&v)[NARR]) {
-    const int k1 = k1_0 + f;
-    const uint32_t ex = (uint32_t)(((uint64_t)k1 * (uint64_t)m) & (L - 1));
-    const C w = to_c<C>(unit_root<SIGN>(tb, ex, log2L));
-#pragma unroll
-    for (int a = 0; a < NARR; ++a) zrow[a * L + size_t(m) * L1 + k1] = cmul(v[a], w);
-  };
+  Pass1Store<C, NARR, SIGN> st{tb, zrow, k1_0, L1, log2L};
   fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
 
 // pass 2: CTA = (n2 block of NF = TILE/L1 values, row, batch item).
 template <class Op, typename C, int LOGL1, int SIGN>
-__global__ void __launch_bounds__(kNT)
+__global__ void __launch_bounds__(kNT, MinBlocks<C>::v)
 tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo,
            int rows_in_tile) {
   constexpr int NARR = Op::NARR;
@@ -128,7 +176,7 @@ tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo,
 #pragma unroll
     for (int a = 0; a < NARR; ++a) v[a] = zrow[a * L + size_t(n2_0 + f) * L1 + m];
   };
-  auto st = [&](int f, int m, C (&v)[NARR]) { op.store(b, row, L2 * m + n2_0 + f, v); };
+  StoreEach<Op, C> st{op, b, row, 0x7fffffff, L2, n2_0};
   fft_rows<C, LOGL1, NF, kNT, SIGN, NARR, MAP_J, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
 
