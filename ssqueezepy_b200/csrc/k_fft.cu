@@ -74,7 +74,11 @@ static int run_tile(const Op& op, int B, int nrows, int log2L, C* Z, size_t zcap
   if (!two_pass<C>(log2L)) return run_single<Op, C, SIGN>(op, B, nrows, log2L, tb, st);
   if (log2L > 22) return (int)cudaErrorInvalidValue;
   const int l2 = log2L / 2, l1 = log2L - l2;
-  const int S = rows_per_tile(zcap, B, Op::NARR, log2L, nrows);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int S = rows_per_tile(zcap, B, Op::NARR, log2L, nrows,
+                              (1 << log2L) / tile_of<C>(), 2 * sms);
   for (int r0 = 0; r0 < nrows; r0 += S) {
     const int rows = (nrows - r0) < S ? (nrows - r0) : S;
     int e;

@@ -10,7 +10,7 @@ namespace ssqb {
 #define SSQB_SQ_G 4
 #endif
 #ifndef SSQB_SQ_U
-#define SSQB_SQ_U 8
+#define SSQB_SQ_U 16
 #endif
 
 template <typename C, class Src>

@@ -2,18 +2,33 @@
 // C-ABI layer. Each returns 0 or a cudaError_t value.
 #pragma once
 #include <cuda_runtime.h>
+#include <cmath>
 #include "ssqb_ops.cuh"
 
 namespace ssqb {
 
-// row tile of the two-pass transform: rows whose intermediate fits in zcap
-// complex elements (at least one row)
-inline int rows_per_tile(size_t zcap_elems, int B, int narr, int log2L, int nrows) {
+// row tile of the two-pass transform: as many rows as the intermediate
+// holds (zcap complex elements, at least one row), then trimmed so that the
+// CTA count of a launch fills whole waves of `slots` resident CTAs
+inline int rows_per_tile(size_t zcap_elems, int B, int narr, int log2L, int nrows,
+                         int ctas_per_row = 0, int slots = 0) {
   const size_t per = (size_t)B * narr * ((size_t)1 << log2L);
   size_t s = per ? zcap_elems / per : 0;
   if (s < 1) s = 1;
   if (s > (size_t)nrows) s = nrows;
   if (s > 65535) s = 65535;
+  if (ctas_per_row > 0 && slots > 0 && s > 1) {
+    double best = 2.0;
+    size_t pick = s;
+    for (size_t r = s; r >= (s + 1) / 2 && r >= 1; --r) {
+      const double c = (double)r * ctas_per_row * B;
+      const double waves = c / slots;
+      const double waste = (std::ceil(waves) - waves) / std::ceil(waves);
+      if (waste < best - 0.02) { best = waste; pick = r; }
+      if (r == 1) break;
+    }
+    s = pick;
+  }
   return (int)s;
 }
 
