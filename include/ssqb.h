@@ -150,6 +150,35 @@ SSQB_API int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, 
               const double* Sfs, const ssqb_bins* bins, double gamma, int precision,
               void* Sx, void* dSx, void* w, uint16_t* idx, int idx_pitch, void* stream);
 
+/* ssqb_cwt without a caller workspace, for callers that cannot allocate
+ * device memory on their call path: for example a plugin inside a host
+ * application that reserves all device memory for its own allocator, or a
+ * streaming loop that cannot afford the implicit device synchronization of
+ * cudaMalloc. No counterpart in ssqueezepy (the reference always allocates
+ * through torch / CuPy).
+ *
+ * Arguments and outputs are those of ssqb_cwt (the caller still provides x,
+ * scales, Wx, idx, ...); the padded-signal spectrum and the two-pass
+ * intermediate live in one fixed scratch array of ssqb_cwt_noalloc_max_bytes()
+ * (16 MiB) of module memory that every device loading the library holds
+ * until the process exits. A call needing more (roughly B * Npad * 48 bytes
+ * for Npad > 2048 with float64 arithmetic, B * Npad * 16 otherwise) fails
+ * with SSQB_EINVAL and a message naming the size. The first call on a device
+ * looks up the array's device address (and builds the twiddle tables); make
+ * that first call before any stream capture. Nothing is allocated or freed.
+ * All calls share the one array: calls that overlap on the GPU (other
+ * streams, other host threads) race and corrupt each other's results; issue
+ * them on one stream or otherwise order them. Nothing in the array needs to
+ * start at zero: each call writes every element it later reads. */
+SSQB_API int ssqb_cwt_noalloc(const void* x, int B, int N, int Npad, int n1, int padtype,
+                              int rpadded, const double* scales, int na,
+                              const ssqb_wavelet* wavelet, double dt, const ssqb_bins* bins,
+                              double gamma, int precision, void* Wx, void* dWx, void* w,
+                              uint16_t* idx, int idx_pitch, void* stream);
+
+/* Size of the fixed scratch array of ssqb_cwt_noalloc, in bytes. */
+SSQB_API size_t ssqb_cwt_noalloc_max_bytes(void);
+
 /* One-integral inverse CWT as a weighted row sum (_cwt.py:479-482 with the
  * scaling of :441-452): x[b, j] = sum_i Re(Wx[b, i, j]) * row_weights[i]
  * + x_mean[b] * mean_weight. x (B, N) real of the given precision; x_mean

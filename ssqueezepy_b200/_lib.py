@@ -49,6 +49,10 @@ SIGNATURES = {
     'ssqb_stft': (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp,
                        ctypes.POINTER(CBins), _d, _i, _vp, _vp, _vp, _vp, _i, _vp]),
     'ssqb_icwt': (_i, [_vp, _vp, _vp, _d, _i, _i, _i, _i, _vp, _vp]),
+    'ssqb_cwt_noalloc': (_i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _i,
+                              ctypes.POINTER(CWavelet), _d, ctypes.POINTER(CBins), _d,
+                              _i, _vp, _vp, _vp, _vp, _i, _vp]),
+    'ssqb_cwt_noalloc_max_bytes': (_sz, []),
 }
 
 _lib = None

@@ -44,6 +44,14 @@ static std::mutex g_mu;
 static bool g_init[256];
 static Tables g_tables[256];
 
+// Scratch of ssqb_cwt_noalloc: module memory, present on every device that
+// loads this library until the process exits. Host code must not use the
+// symbol's name as a device address; the address comes from
+// cudaGetSymbolAddress, once per device (g_noalloc_ptr).
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static void* g_noalloc_ptr[256];
+
 static int fail(int code, const std::string& msg) {
   t_err = msg;
   return code;
@@ -383,5 +391,44 @@ int ssqb_icwt(const void* Wx, const double* row_weights, const double* x_mean,
   if (e) return cuda_fail((cudaError_t)e, "icwt launch");
   return SSQB_OK;
 }
+
+int ssqb_cwt_noalloc(const void* x, int B, int N, int Npad, int n1, int padtype,
+                     int rpadded, const double* scales, int na,
+                     const ssqb_wavelet* wavelet, double dt, const ssqb_bins* bins,
+                     double gamma, int precision, void* Wx, void* dWx, void* w,
+                     uint16_t* idx, int idx_pitch, void* stream) {
+  if (B < 1 || na < 1 || !is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
+    return ssqb_cwt(x, B, N, Npad, n1, padtype, rpadded, scales, na, wavelet, dt, bins,
+                    gamma, precision, Wx, dWx, w, idx, idx_pitch, nullptr, 0, stream);
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  const size_t need = xhat_bytes(B, Npad) + min_z_bytes(B, Npad, precision);
+  if (need > kNoAllocScratchBytes)
+    return fail(SSQB_EINVAL,
+                "ssqb_cwt_noalloc: this call needs " + std::to_string(need) +
+                    " bytes of scratch, more than its fixed " +
+                    std::to_string(kNoAllocScratchBytes) +
+                    " bytes; use ssqb_cwt with a caller workspace");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 256) return fail(SSQB_EINVAL, "device ordinal out of range");
+  void* scratch;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      if ((e = cudaGetSymbolAddress(&p, g_noalloc_scratch)))
+        return cuda_fail(e, "symbol noalloc scratch");
+      g_noalloc_ptr[dev] = p;
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  return ssqb_cwt(x, B, N, Npad, n1, padtype, rpadded, scales, na, wavelet, dt, bins, gamma,
+                  precision, Wx, dWx, w, idx, idx_pitch, scratch, kNoAllocScratchBytes,
+                  stream);
+}
+
+size_t ssqb_cwt_noalloc_max_bytes(void) { return kNoAllocScratchBytes; }
 
 }  // extern "C"
