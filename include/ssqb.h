@@ -187,6 +187,54 @@ SSQB_API int ssqb_icwt(const void* Wx, const double* row_weights, const double* 
                        double mean_weight, int B, int na, int N, int precision,
                        void* x, void* stream);
 
+/* ---- batches of signals of uneven length ---------------------------------
+ * ssqueezepy transforms a 2D input of equal-length rows (_cwt.py:270-271) and
+ * squeezes it one signal at a time (ssqueezing.py:210-214); signals of
+ * different lengths need one call each. These entry points take many
+ * signals at once, packed end to end, each described by an ssqb_sig.
+ * Offsets count elements of the packed arrays. All signals of one
+ * ssqb_cwt_batch call share the padded length Npad (group them by
+ * p2up(N), utils/common.py:32-51); ssqb_squeeze_batch takes any mix. */
+typedef struct ssqb_sig {
+  int64_t x_off;          /* first sample of the signal in x */
+  int64_t out_off;        /* first element of its (na, N) block in Wx and Tx */
+  int64_t idx_off;        /* first element of its (na, idx_pitch) block in idx */
+  const double* scales;   /* device, (na) float64 */
+  const double* weights;  /* device, (na) float64 squeeze row weights */
+  int32_t N, n1, na, idx_pitch;
+  int32_t mode, idx1, flipud, nbins;  /* bin mapping as in ssqb_bins; nbins = na */
+  double p[4];
+} ssqb_sig;
+
+/* Workspace bytes of ssqb_cwt_batch: the float64 spectra of all nsig
+ * signals plus a bounded intermediate (signals are processed in chunks that
+ * fit it). */
+SSQB_API size_t ssqb_cwt_batch_workspace_bytes(int nsig, int Npad, int precision);
+
+/* ssqb_cwt with bin index for nsig float32 signals of one padded length:
+ * x packed float32; Wx complex64 and idx uint16 written at each signal's
+ * offsets. `sigs` is a host array of the descriptors, used to check the
+ * arguments and size the launches; `sigs_dev` holds the same descriptors in
+ * device memory and is what the kernels read. precision SSQB_F32 or
+ * SSQB_F32X. A CUDA graph may capture the call once one call has run on the
+ * device. */
+SSQB_API int ssqb_cwt_batch(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_dev,
+                            int nsig, int Npad, int padtype, const ssqb_wavelet* wavelet,
+                            double dt, double gamma, int precision, void* Wx, uint16_t* idx,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* Number of kernel launches of one ssqb_cwt_batch call with these
+ * descriptors (host array) and workspace size; -1 on bad arguments. Queries
+ * the current device's SM count; no reference counterpart. */
+SSQB_API int ssqb_cwt_batch_launches(const ssqb_sig* sigs, int nsig, int Npad, int precision,
+                                     size_t workspace_bytes);
+
+/* ssqb_squeeze over nsig signals of any lengths, one launch: Tx (complex64)
+ * at each signal's out_offset, from its Wx block, idx block and weights. */
+SSQB_API int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_sig* sigs,
+                                const ssqb_sig* sigs_dev, int nsig, int precision, void* Tx,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,13 +12,15 @@ from ._transforms import (cwt, ssq_cwt, icwt, stft, ssq_stft, ssqueeze,
 from ._params import (p2up, process_scales, make_scales, cwt_scalebounds,
                       center_frequency, adm_ssq, logscale_transition_idx,
                       infer_scaletype, nv_from_scales)
+from ._batch import SsqCwtBatch, ssq_cwt_batch
 from . import _lib
 
 __version__ = '0.1.0'
 __all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
            'phase_cwt', 'phase_stft', 'Wavelet', 'configure', 'p2up', 'process_scales',
            'make_scales', 'cwt_scalebounds', 'center_frequency', 'adm_ssq',
-           'logscale_transition_idx', 'infer_scaletype', 'nv_from_scales']
+           'logscale_transition_idx', 'infer_scaletype', 'nv_from_scales',
+           'SsqCwtBatch', 'ssq_cwt_batch']
 
 
 def wavs():

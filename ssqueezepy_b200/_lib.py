@@ -53,7 +53,21 @@ SIGNATURES = {
                               ctypes.POINTER(CWavelet), _d, ctypes.POINTER(CBins), _d,
                               _i, _vp, _vp, _vp, _vp, _i, _vp]),
     'ssqb_cwt_noalloc_max_bytes': (_sz, []),
+    'ssqb_cwt_batch_workspace_bytes': (_sz, [_i, _i, _i]),
+    'ssqb_cwt_batch': (_i, [_vp, _vp, _vp, _i, _i, _i, ctypes.POINTER(CWavelet), _d, _d,
+                            _i, _vp, _vp, _vp, _sz, _vp]),
+    'ssqb_cwt_batch_launches': (_i, [_vp, _i, _i, _i, _sz]),
+    'ssqb_squeeze_batch': (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),
 }
+
+# numpy layout of `ssqb_sig` (one signal of a batch of uneven lengths)
+SIG_DTYPE = np.dtype([('x_off', np.int64), ('out_off', np.int64), ('idx_off', np.int64),
+                      ('scales', np.uint64), ('weights', np.uint64),
+                      ('N', np.int32), ('n1', np.int32), ('na', np.int32),
+                      ('idx_pitch', np.int32), ('mode', np.int32), ('idx1', np.int32),
+                      ('flipud', np.int32), ('nbins', np.int32), ('p', np.float64, (4,))],
+                     align=True)
+assert SIG_DTYPE.itemsize == 104
 
 _lib = None
 _lock = threading.Lock()

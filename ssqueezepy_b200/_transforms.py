@@ -106,7 +106,7 @@ def _dev_f64(a, dev):
 # (wavelet, N, scheme) always yields the same float64 parameters, so they are
 # computed once. Device copies are kept per device.
 _PLANS = {}
-_PLAN_MAX = 64
+_PLAN_MAX = 1024
 
 
 def _wkey(wavelet):

@@ -1,6 +1,7 @@
 // C-ABI layer: argument checks, per-device tables, dispatch to launchers.
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -144,6 +145,52 @@ static size_t min_z_bytes(int B, int Npad, int precision) {
   const size_t a = two_pass<double2>(m) ? (size_t)B * Npad * sizeof(double2) : 0;
   const size_t c = cwt_two_pass(m, precision) ? (size_t)B * 2 * Npad * csize(precision) : 0;
   return a > c ? a : c;
+}
+
+// ---- batches of uneven lengths ------------------------------------------------
+static_assert(sizeof(ssqb_sig) == sizeof(SigDesc), "ssqb_sig / SigDesc layout");
+static_assert(offsetof(ssqb_sig, scales) == offsetof(SigDesc, scales), "ssqb_sig layout");
+static_assert(offsetof(ssqb_sig, N) == offsetof(SigDesc, N), "ssqb_sig layout");
+static_assert(offsetof(ssqb_sig, mode) == offsetof(SigDesc, mode), "ssqb_sig layout");
+static_assert(offsetof(ssqb_sig, p) == offsetof(SigDesc, p0), "ssqb_sig layout");
+
+// bound of the batch intermediate: chunks of signals and rows that fit it
+constexpr size_t kBatchZBytes = (size_t)64 << 20;
+
+static size_t batch_z_bytes(int Npad, int precision) {
+  const size_t one = min_z_bytes(1, Npad, precision);
+  return one == 0 ? 0 : (one > kBatchZBytes ? one : kBatchZBytes);
+}
+
+// host-side check of the descriptors; `Npad` > 0 also checks the padding
+// geometry of each signal against it
+static int check_sigs(const ssqb_sig* s, int nsig, int Npad, bool need_scales,
+                      bool need_weights, int* max_na, int* max_N) {
+  if (!s) return fail(SSQB_EINVAL, "sigs is NULL");
+  if (nsig < 1 || nsig > 65535) return fail(SSQB_EINVAL, "nsig must be in [1, 65535]");
+  int mna = 0, mN = 0;
+  for (int i = 0; i < nsig; ++i) {
+    const ssqb_sig& d = s[i];
+    const std::string at = "signal " + std::to_string(i) + ": ";
+    if (d.N < 1 || d.na < 1 || d.na > 65535)
+      return fail(SSQB_EINVAL, at + "N must be >= 1 and na in [1, 65535]");
+    if (d.x_off < 0 || d.out_off < 0 || d.idx_off < 0)
+      return fail(SSQB_EINVAL, at + "negative offset");
+    if (d.idx_pitch < d.N) return fail(SSQB_EINVAL, at + "idx_pitch smaller than N");
+    if (Npad > 0 && (d.N > Npad || d.n1 < 0 || d.n1 + d.N > Npad))
+      return fail(SSQB_EINVAL, at + "bad padding geometry");
+    if (need_scales && !d.scales) return fail(SSQB_EINVAL, at + "scales is NULL");
+    if (need_weights && !d.weights) return fail(SSQB_EINVAL, at + "weights is NULL");
+    ssqb_bins b{d.mode, d.idx1, d.flipud, d.nbins, {d.p[0], d.p[1], d.p[2], d.p[3]}};
+    BinDev bd;
+    const int r = check_bins(&b, d.na, &bd);
+    if (r) return fail(r, at + t_err);
+    if (d.na > mna) mna = d.na;
+    if (d.N > mN) mN = d.N;
+  }
+  *max_na = mna;
+  *max_N = mN;
+  return SSQB_OK;
 }
 
 }  // namespace ssqb
@@ -430,5 +477,108 @@ int ssqb_cwt_noalloc(const void* x, int B, int N, int Npad, int n1, int padtype,
 }
 
 size_t ssqb_cwt_noalloc_max_bytes(void) { return kNoAllocScratchBytes; }
+
+size_t ssqb_cwt_batch_workspace_bytes(int nsig, int Npad, int precision) {
+  if (nsig < 1 || !is_pow2(Npad)) return 0;
+  return xhat_bytes(nsig, Npad) + batch_z_bytes(Npad, precision);
+}
+
+int ssqb_cwt_batch(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_dev, int nsig,
+                   int Npad, int padtype, const ssqb_wavelet* wavelet, double dt,
+                   double gamma, int precision, void* Wx, uint16_t* idx, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  if (!x || !sigs_dev || !Wx || !idx || !workspace)
+    return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (precision != SSQB_F32 && precision != SSQB_F32X)
+    return fail(SSQB_EUNSUPPORTED, "batches take float32 data: precision SSQB_F32 or SSQB_F32X");
+  if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
+    return fail(SSQB_EUNSUPPORTED, "Npad must be a power of two in [8, 2^22]");
+  if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
+  if (!(dt > 0)) return fail(SSQB_EINVAL, "dt must be > 0");
+  int max_na = 0, max_N = 0;
+  int r = check_sigs(sigs, nsig, Npad, true, false, &max_na, &max_N);
+  if (r) return r;
+  WavDev wd;
+  r = check_wavelet(wavelet, &wd);
+  if (r) return r;
+  const size_t xb = xhat_bytes(nsig, Npad);
+  const size_t need = xb + min_z_bytes(1, Npad, precision);
+  if (workspace_bytes < need)
+    return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                     " bytes");
+  Tables tb;
+  r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  const SigDesc* dd = reinterpret_cast<const SigDesc*>(sigs_dev);
+  double2* xh = (double2*)workspace;
+  unsigned char* zb = (unsigned char*)workspace + xb;
+  const size_t zbytes = workspace_bytes - xb;
+  int e = run_xhat_batch_f32(x, dd, nsig, Npad, padtype, xh, (double2*)zb,
+                             zbytes / sizeof(double2), tb, st);
+  if (e) return cuda_fail((cudaError_t)e, "x_hat launch");
+  const int m = ilog2i(Npad);
+  const double h = (2 * M_PI) / Npad;
+  if (precision == SSQB_F32X) {
+    CwtBatchOp<double2, float2> op{xh, dd, wd, Npad, h, 1.0 / dt, 1.0 / Npad, gamma,
+                                   (float2*)Wx, idx, tb.status};
+    e = run_cwt_batch_f32x(op, nsig, max_na, m, (double2*)zb, zbytes / sizeof(double2), tb,
+                           st);
+  } else {
+    CwtBatchOp<float2, float2> op{xh, dd, wd, Npad, h, 1.0 / dt, (float)(1.0 / Npad), gamma,
+                                  (float2*)Wx, idx, tb.status};
+    e = run_cwt_batch_f32(op, nsig, max_na, m, (float2*)zb, zbytes / sizeof(float2), tb, st);
+  }
+  if (e) return cuda_fail((cudaError_t)e, "cwt launch");
+  return SSQB_OK;
+}
+
+int ssqb_cwt_batch_launches(const ssqb_sig* sigs, int nsig, int Npad, int precision,
+                            size_t workspace_bytes) {
+  if (precision != SSQB_F32 && precision != SSQB_F32X) return -1;
+  if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22)) return -1;
+  int max_na = 0, max_N = 0;
+  if (check_sigs(sigs, nsig, Npad, false, false, &max_na, &max_N)) return -1;
+  const size_t xb = xhat_bytes(nsig, Npad);
+  if (workspace_bytes < xb + min_z_bytes(1, Npad, precision)) return -1;
+  const size_t zbytes = workspace_bytes - xb;
+  Tables tb{};
+  int count = 0;
+  set_launch_counter(&count);
+  run_xhat_batch_f32(nullptr, nullptr, nsig, Npad, 1, nullptr, nullptr,
+                     zbytes / sizeof(double2), tb, 0);
+  const int m = ilog2i(Npad);
+  if (precision == SSQB_F32X) {
+    CwtBatchOp<double2, float2> op{};
+    run_cwt_batch_f32x(op, nsig, max_na, m, nullptr, zbytes / sizeof(double2), tb, 0);
+  } else {
+    CwtBatchOp<float2, float2> op{};
+    run_cwt_batch_f32(op, nsig, max_na, m, nullptr, zbytes / sizeof(float2), tb, 0);
+  }
+  set_launch_counter(nullptr);
+  return count;
+}
+
+int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_sig* sigs,
+                       const ssqb_sig* sigs_dev, int nsig, int precision, void* Tx,
+                       void* stream) {
+  if (!Wx || !idx || !sigs_dev || !Tx) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (precision != SSQB_F32 && precision != SSQB_F32X)
+    return fail(SSQB_EUNSUPPORTED, "batches take float32 data: precision SSQB_F32 or SSQB_F32X");
+  int max_na = 0, max_N = 0;
+  int r = check_sigs(sigs, nsig, 0, false, true, &max_na, &max_N);
+  if (r) return r;
+  const size_t smem = (size_t)max_na * 8 * sizeof(float2) + (size_t)max_na * sizeof(float);
+  if (smem > 227 * 1024)
+    return fail(SSQB_EUNSUPPORTED, "too many bins for the shared-memory squeeze");
+  Tables tb;
+  r = get_tables(&tb);
+  if (r) return r;
+  int e = run_squeeze_batch_f32((const float2*)Wx, idx,
+                                reinterpret_cast<const SigDesc*>(sigs_dev), nsig, max_na,
+                                max_N, (float2*)Tx, tb.status, (cudaStream_t)stream);
+  if (e) return cuda_fail((cudaError_t)e, "squeeze launch");
+  return SSQB_OK;
+}
 
 }  // extern "C"

@@ -51,6 +51,21 @@ static int run_sq(const C* Wx, int src_kind, const void* src, int idx_pitch,
   }
 }
 
+int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* desc,
+                          int nsig, int max_na, int max_N, float2* Tx, int* status,
+                          cudaStream_t st) {
+  if (int* c = launch_counter()) return ++*c, 0;
+  constexpr int G = SSQB_SQ_G, U = SSQB_SQ_U, CW = 32 / G;
+  const size_t smem = (size_t)max_na * CW * sizeof(float2) + (size_t)max_na * sizeof(float);
+  auto k = squeeze_batch_kernel<float2, G, U>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  dim3 grid((max_N + CW - 1) / CW, nsig);
+  k<<<grid, 32, smem, st>>>(Wx, idx, desc, Tx, status);
+  return cudaGetLastError();
+}
+
 int run_squeeze_f32(const float2* Wx, int src_kind, const void* src, int idx_pitch,
                     const double* sfs, const BinDev& bins, double gamma, const double* cst,
                     int B, int na, int N, int nbins, float2* Tx, int* status,

@@ -71,4 +71,21 @@ int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, int idx_pi
 int run_icwt(const void* Wx, const double* w, const double* x_mean, double mean_weight,
              int B, int na, int N, int precision, void* x, cudaStream_t st);
 
+// count launches of this host thread into *c instead of launching (NULL:
+// launch again)
+void set_launch_counter(int* c);
+int* launch_counter();
+
+// batches of uneven lengths sharing one padded length (float32 data)
+int run_xhat_batch_f32(const float* x, const SigDesc* desc, int nsig, int Npad, int padtype,
+                       double2* xh, double2* Z, size_t zcap, const Tables& tb,
+                       cudaStream_t st);
+int run_cwt_batch_f32x(const CwtBatchOp<double2, float2>& op, int nsig, int max_na,
+                       int log2L, double2* Z, size_t zcap, const Tables& tb, cudaStream_t st);
+int run_cwt_batch_f32(const CwtBatchOp<float2, float2>& op, int nsig, int max_na, int log2L,
+                      float2* Z, size_t zcap, const Tables& tb, cudaStream_t st);
+int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* desc,
+                          int nsig, int max_na, int max_N, float2* Tx, int* status,
+                          cudaStream_t st);
+
 }  // namespace ssqb

@@ -65,9 +65,10 @@ struct WSrc {
 // between them), so every bin still receives its rows in ascending order.
 // Loads for U row groups are issued before their updates.
 template <typename C, class Src, int G, int U>
-__global__ void __launch_bounds__(32)
-squeeze_kernel(const C* __restrict__ Wx, Src src, const double* __restrict__ cst,
-               int na, int N, int nbins, C* __restrict__ Tx, int* status) {
+__device__ __forceinline__ void squeeze_body(const C* __restrict__ Wx, const Src& src,
+                                             const double* __restrict__ cst, int na, int N,
+                                             int nbins, C* __restrict__ Tx, int* status,
+                                             int b, int tile) {
   typedef typename RealOf<C>::type T;
   constexpr int CW = 32 / G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -75,8 +76,7 @@ squeeze_kernel(const C* __restrict__ Wx, Src src, const double* __restrict__ cst
   T* cs = reinterpret_cast<T*>(acc + (size_t)nbins * CW);   // [na]
   const int lane = threadIdx.x;
   const int g = lane / CW, c = lane % CW;
-  const int b = blockIdx.y;
-  const int j = blockIdx.x * CW + c;
+  const int j = tile * CW + c;
   const bool live = j < N;
   for (int k = lane; k < nbins * CW; k += 32) acc[k] = mk((T)0, (T)0);
   for (int i = lane; i < na; i += 32) cs[i] = (T)cst[i];
@@ -117,12 +117,32 @@ squeeze_kernel(const C* __restrict__ Wx, Src src, const double* __restrict__ cst
     }
   }
   __syncwarp();
-  C* out = Tx + (size_t)b * nbins * N + blockIdx.x * CW;
-  const int ncol = min(CW, N - (int)blockIdx.x * CW);
+  C* out = Tx + (size_t)b * nbins * N + tile * CW;
+  const int ncol = min(CW, N - tile * CW);
   for (int e = lane; e < nbins * CW; e += 32) {
     const int k = e / CW, cc = e % CW;
     if (cc < ncol) out[(size_t)k * N + cc] = acc[e];
   }
+}
+
+template <typename C, class Src, int G, int U>
+__global__ void __launch_bounds__(32)
+squeeze_kernel(const C* __restrict__ Wx, Src src, const double* __restrict__ cst,
+               int na, int N, int nbins, C* __restrict__ Tx, int* status) {
+  squeeze_body<C, Src, G, U>(Wx, src, cst, na, N, nbins, Tx, status, blockIdx.y, blockIdx.x);
+}
+
+// Batches of uneven lengths: signal blockIdx.y per its descriptor; column
+// tiles past its length return at once.
+template <typename C, int G, int U>
+__global__ void __launch_bounds__(32)
+squeeze_batch_kernel(const C* __restrict__ Wx, const uint16_t* __restrict__ idx,
+                     const SigDesc* __restrict__ desc, C* __restrict__ Tx, int* status) {
+  const SigDesc& d = desc[blockIdx.y];
+  if ((int)blockIdx.x * (32 / G) >= d.N) return;
+  IdxSrc<C> src{idx + d.idx_off, d.idx_pitch, d.N};
+  squeeze_body<C, IdxSrc<C>, G, U>(Wx + d.out_off, src, d.weights, d.na, d.N, d.nbins,
+                                   Tx + d.out_off, status, 0, blockIdx.x);
 }
 
 }  // namespace ssqb

@@ -34,6 +34,17 @@ struct BinDev {
   double p0, p1, p2, p3;  // log: vlmin, dvl | piecewise: vlmin0, vlmin1, dvl0, dvl1 | lin: vmin, dv
 };
 
+// Per-signal descriptor of a batch of uneven lengths (same layout as
+// ssqb_sig in include/ssqb.h).
+struct SigDesc {
+  long long x_off, out_off, idx_off;
+  const double* scales;
+  const double* weights;
+  int N, n1, na, idx_pitch;
+  int mode, idx1, flipud, nbins;
+  double p0, p1, p2, p3;
+};
+
 constexpr uint16_t kNoBin = 0xFFFF;
 constexpr double kTwoPi = 6.283185307179586;  // the literal of algos.py:867
 
@@ -206,9 +217,11 @@ template <typename TX>
 struct XhatOp {
   static constexpr int NARR = 1;
   static constexpr bool kDirect = true;
+  static constexpr bool kBatch = false;
   const TX* x;       // (B, N)
   double2* xh;       // (B, Npad)
   int N, Npad, n1, padtype;
+  __device__ XhatOp bind(int) const { return *this; }
   __device__ int rows() const { return 1; }
   __device__ void load(int b, int, int k, double2 (&v)[1]) const {
     const int s = pad_src((long long)k - n1, N, padtype);
@@ -235,6 +248,7 @@ struct CwtOp {
   typedef typename RealOf<OC>::type OT;
   static constexpr int NARR = 2;
   static constexpr bool kDirect = true;
+  static constexpr bool kBatch = false;
   const double2* xh;      // (B, Npad) float64
   const double* scales;   // (na)
   WavDev wav;
@@ -250,6 +264,7 @@ struct CwtOp {
   uint16_t* idx;          // optional bin index, (B, na, idx_pitch)
   int idx_pitch;
   int* status;
+  __device__ CwtOp bind(int) const { return *this; }
   __device__ int rows() const { return na; }
   __device__ void load(int b, int row, int k, C (&v)[2]) const {
     const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
@@ -289,6 +304,7 @@ struct StftOp {
   typedef typename RealOf<OC>::type OT;
   static constexpr int NARR = 1;
   static constexpr bool kDirect = false;
+  static constexpr bool kBatch = false;
   const TX* x;             // (B, N)
   const double* win;       // (n_fft)
   const double* dwin;      // (n_fft), already times fs
@@ -302,6 +318,7 @@ struct StftOp {
   uint16_t* idx;           // (B, L/2+1, idx_pitch)
   int idx_pitch;
   int* status;
+  __device__ StftOp bind(int) const { return *this; }
   __device__ int rows() const { return nframes; }
   __device__ void load(int b, int t, int m, C (&v)[1]) const {
     const int q = modulated ? ((m + s21) & (L - 1)) : m;
@@ -331,6 +348,49 @@ struct StftOp {
       if (idx) idx[((size_t)b * nrow + n) * idx_pitch + t] = k;
       if (w) w[o] = (OT)wv;
     }
+  }
+};
+
+// ---- batches of uneven lengths (one padded length per launch) ---------------
+// bind(b) turns the batch op into the single-signal op of signal b, with its
+// pointers already offset (the kernels then call it with batch index 0).
+template <typename TX>
+struct XhatBatchOp {
+  static constexpr int NARR = 1;
+  static constexpr bool kDirect = true;
+  static constexpr bool kBatch = true;
+  const TX* x;
+  double2* xh;              // (nsig, Npad)
+  const SigDesc* desc;
+  int Npad, padtype;
+  __device__ XhatOp<TX> bind(int b) const {
+    const SigDesc& d = desc[b];
+    return XhatOp<TX>{x + d.x_off, xh + (size_t)b * Npad, d.N, Npad, d.n1, padtype};
+  }
+};
+
+template <typename C, typename OC>
+struct CwtBatchOp {
+  typedef typename RealOf<C>::type T;
+  static constexpr int NARR = 2;
+  static constexpr bool kDirect = true;
+  static constexpr bool kBatch = true;
+  const double2* xh;        // (nsig, Npad)
+  const SigDesc* desc;
+  WavDev wav;
+  int Npad;
+  double h, inv_dt;
+  T inv_npad;
+  double gamma;
+  OC* Wx;
+  uint16_t* idx;
+  int* status;
+  __device__ CwtOp<C, OC> bind(int b) const {
+    const SigDesc& d = desc[b];
+    const BinDev bd{d.mode, d.idx1, d.flipud, d.nbins, d.p0, d.p1, d.p2, d.p3};
+    return CwtOp<C, OC>{xh + (size_t)b * Npad, d.scales, wav, bd, d.na, d.N, Npad, d.n1,
+                        h, inv_dt, inv_npad, gamma, Wx + d.out_off, nullptr, nullptr,
+                        idx + d.idx_off, d.idx_pitch, status};
   }
 };
 

@@ -98,27 +98,30 @@ tile_single(Op op, Tables tb) {
 #pragma unroll
   for (int a = 0; a < NARR; ++a) bufs[a] = base + a * LY::ARR;
   C* const(&buf)[NARR] = bufs;
-  const int b = blockIdx.z;
+  const auto bop = op.bind(blockIdx.z);  // per-signal op (batches of uneven lengths)
+  const int b = Op::kBatch ? 0 : blockIdx.z;
   const int row0 = blockIdx.x * NF;
-  const int nrows = op.rows();
+  const int nrows = bop.rows();
+  if (row0 >= nrows) return;
   auto ld = [&](int f, int m, C (&v)[NARR]) {
     if (row0 + f < nrows) {
-      op.load(b, row0 + f, m, v);
+      bop.load(b, row0 + f, m, v);
     } else {
 #pragma unroll
       for (int a = 0; a < NARR; ++a)
         v[a] = mk((typename RealOf<C>::type)0, (typename RealOf<C>::type)0);
     }
   };
+  typedef decltype(op.bind(0)) BOp;
   if constexpr (Op::kDirect) {
-    StoreEach<Op, C> st{op, b, row0, nrows, 1, 0};
+    StoreEach<BOp, C> st{bop, b, row0, nrows, 1, 0};
     fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, true>(buf, seg_table<C>(tb), ld, st);
   } else {
-    StoreEach<Op, C> st{op, b, row0, nrows, 1, 0};
+    StoreEach<BOp, C> st{bop, b, row0, nrows, 1, 0};
     fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, false>(buf, seg_table<C>(tb), ld, st);
     for (int e = threadIdx.x; e < TILE; e += kNT) {
       const int f = e % NF, n = e / NF;  // rows fastest: coalesced (row, n) outputs
-      if (row0 + f < nrows) op.template store_smem<LY>(b, row0 + f, n, buf, f);
+      if (row0 + f < nrows) bop.template store_smem<LY>(b, row0 + f, n, buf, f);
     }
   }
 }
@@ -140,12 +143,14 @@ tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_
   for (int a = 0; a < NARR; ++a) bufs[a] = base + a * LY::ARR;
   C* const(&buf)[NARR] = bufs;
   const int L1 = 1 << (log2L - LOGL2);
-  const int b = blockIdx.z;
+  const auto bop = op.bind(blockIdx.z);
+  const int b = Op::kBatch ? 0 : blockIdx.z;
   const int row = row_lo + blockIdx.y;
+  if (row >= bop.rows()) return;  // signals with fewer rows (uneven batches)
   const int k1_0 = blockIdx.x * NF;
   const size_t L = size_t(1) << log2L;
-  C* zrow = Z + (size_t(b) * rows_in_tile + blockIdx.y) * NARR * L;
-  auto ld = [&](int f, int m, C (&v)[NARR]) { op.load(b, row, k1_0 + f + L1 * m, v); };
+  C* zrow = Z + (size_t(blockIdx.z) * rows_in_tile + blockIdx.y) * NARR * L;
+  auto ld = [&](int f, int m, C (&v)[NARR]) { bop.load(b, row, k1_0 + f + L1 * m, v); };
   Pass1Store<C, NARR, SIGN> st{tb, zrow, k1_0, L1, log2L};
   fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
@@ -167,16 +172,19 @@ tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo,
   for (int a = 0; a < NARR; ++a) bufs[a] = base + a * LY::ARR;
   C* const(&buf)[NARR] = bufs;
   const int L2 = 1 << (log2L - LOGL1);
-  const int b = blockIdx.z;
+  const auto bop = op.bind(blockIdx.z);
+  const int b = Op::kBatch ? 0 : blockIdx.z;
   const int row = row_lo + blockIdx.y;
+  if (row >= bop.rows()) return;
   const int n2_0 = blockIdx.x * NF;
   const size_t L = size_t(1) << log2L;
-  const C* zrow = Z + (size_t(b) * rows_in_tile + blockIdx.y) * NARR * L;
+  const C* zrow = Z + (size_t(blockIdx.z) * rows_in_tile + blockIdx.y) * NARR * L;
   auto ld = [&](int f, int m, C (&v)[NARR]) {
 #pragma unroll
     for (int a = 0; a < NARR; ++a) v[a] = zrow[a * L + size_t(n2_0 + f) * L1 + m];
   };
-  StoreEach<Op, C> st{op, b, row, 0x7fffffff, L2, n2_0};
+  typedef decltype(op.bind(0)) BOp;
+  StoreEach<BOp, C> st{bop, b, row, 0x7fffffff, L2, n2_0};
   fft_rows<C, LOGL1, NF, kNT, SIGN, NARR, MAP_J, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
 
