@@ -209,18 +209,17 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    clk = Clocks(local) if rank == 0 else None  # samples through every timed leg
     for _ in range(max(args.warmup, 3)):
         step()
     assert L.device_status() == 0
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)]
            for _ in range(args.steps)]
-    clk = Clocks(local) if rank == 0 else None
     barrier()
     for k in range(args.steps):
         flush.zero_()  # write 252 MB > L2 between timed steps (outside events)
         step(evs[k])
     barrier()
-    clocks = clk.stop() if clk else None
     cwt_ms = [e[0].elapsed_time(e[1]) for e in evs]
     sq_ms = [e[1].elapsed_time(e[2]) for e in evs]
     step_ms = float(np.sum(cwt_ms) + np.sum(sq_ms)) / args.steps
@@ -237,9 +236,16 @@ def run_ours(args):
     else:
         e2e_value = run_e2e(sb, torch, dist, x_np, na, N, st, world, dev, barrier,
                             args)
+    Tx_keep = Tx[0].cpu().numpy() if rank == 0 else None
+    Wx_keep = Wx[0].cpu().numpy() if rank == 0 else None
+    batched = None
+    if not args.no_batch:
+        del Wx, Tx, idx, ws
+        batched = run_batched(args, torch, dev, world, barrier, flush)
+    clocks = clk.stop() if clk else None
     if rank == 0:
         emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
-             launches, clocks, sc, f, const, Tx, Wx)
+             launches, clocks, sc, f, const, Tx_keep, Wx_keep, batched)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -268,8 +274,92 @@ def run_e2e(sb, torch, dist, x_np, na, N, st, world, dev, barrier, args):
     return world * N / (float(e2e_ms.item()) * 1e-3)
 
 
+def run_batched(args, torch, dev, world, barrier, flush):
+    """256 float32 signals of lengths uniform in [4096, 65536] (seeded chirp
+    mixtures), Morlet mu=6, nv=32 log-piecewise: one SsqCwtBatch plan (a
+    CUDA graph per step) against one public ssq_cwt call per signal, both with
+    inputs resident on the device."""
+    import torch.distributed as dist
+    import ssqueezepy_b200 as sb
+    from ssqueezepy_b200._batch import SsqCwtBatch
+    from ssqueezepy_b200 import _signals as S
+    rank = int(os.environ.get('RANK', 0))
+    xs = [x.astype(np.float32) for x in
+          S.uneven_batch(args.batch, 4096, 65536, seed=1234 + rank)]
+    lengths = [len(x) for x in xs]
+    wav = ('morlet', {'mu': 6., 'dtype': 'float32'})
+    plan = SsqCwtBatch(lengths, wavelet=wav, graph=True, device=dev)
+    plan.load(xs)
+    st = torch.cuda.current_stream()
+    for _ in range(max(args.warmup, 3)):
+        plan.run()
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for e in evs:
+        flush.zero_()
+        e[0].record(st)
+        plan.run()
+        e[1].record(st)
+    barrier()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    # the same signals, one public ssq_cwt call each (inputs on the device)
+    xd = [torch.as_tensor(x, device=dev) for x in xs]
+    for x in xd:  # host parameter plans for every length, kernels warm
+        sb.ssq_cwt(x, wav, scales='log-piecewise', nv=32)
+    barrier()
+    psteps = max(1, min(args.steps, 3))
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.zero_()
+    p0.record(st)
+    for _ in range(psteps):
+        for x in xd:
+            sb.ssq_cwt(x, wav, scales='log-piecewise', nv=32)
+    p1.record(st)
+    barrier()
+    plain_ms = p0.elapsed_time(p1) / psteps
+    t = torch.tensor([ms, plain_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, plain_ms = float(t[0]), float(t[1])
+    nas = plan.sig_np['na'].astype(np.int64)
+    Ns = plan.sig_np['N'].astype(np.int64)
+    tot = int(Ns.sum())
+    alg = int(((4 + 16 * nas) * Ns).sum())
+    hbm, src = peaks()
+    tx_err = None
+    if rank == 0 and not args.no_cpu:
+        from oracle import ssq_oracle as O
+        outs = plan.outputs()
+        errs = []
+        for i in (int(np.argmin(Ns)), int(np.argmax(Ns))):
+            To, _, _ = O.ssq_cwt(xs[i].astype(np.float64), 'morlet', (6.,),
+                                 plan.scales64[i], plan.ssq_freqs[i][::-1].copy(),
+                                 plan.weights64[i])
+            Tg = outs[i][0].cpu().numpy()
+            errs.append(float(np.linalg.norm(Tg - To) / np.linalg.norm(To)))
+        tx_err = max(errs)
+    return {
+        "workload": "ssq_cwt batch of %d float32 signals, N uniform in [4096, 65536] "
+                    "(sum N = %d), Morlet mu=6 nv=32 log-piecewise (%d-%d rows), "
+                    "reflect; one SsqCwtBatch plan replayed as a CUDA graph"
+                    % (len(xs), tot, nas.min(), nas.max()),
+        "value": world * tot / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+        "plain_value": world * tot / (plain_ms * 1e-3), "plain_ms_per_step": plain_ms,
+        "speedup_vs_plain": plain_ms / ms,
+        "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": hbm,
+                     "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / hbm,
+                     "peak_source": src,
+                     "bytes": "sum_i N_i (4 + 16 na_i): read x, write Wx and Tx"},
+        "gpu_launches": plan.launches * args.steps,
+        "l2": "252 MB buffer written between timed steps; outputs %.1f GB"
+              % (plan.n_out * 16 / 1e9),
+        "Tx_rel_l2_vs_oracle_shortest_longest": tx_err,
+    }
+
+
 def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
-         launches, clocks, sc, f, const, Tx, Wx):
+         launches, clocks, sc, f, const, Tg, Wg, batched=None):
     hbm, src = peaks()
     if True:
         alg_cwt = (4 + 8 * na) * N          # read x, write Wx
@@ -302,6 +392,8 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
             "gpu_launches": launches * args.steps,
             "clocks": clocks,
         }
+        if batched is not None:
+            line["batched"] = batched
         if world == 1 and not args.no_cpu:
             t0 = time.perf_counter()
             To, Wo, _ = oracle_step(chirp_signal(N, seed=0), sc, f, const)
@@ -310,7 +402,6 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
                 "value": N / tc, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                 "sample": "one full N=%d ssq_cwt, float64 numpy/scipy restatement, "
                           "scipy.fft workers=%d" % (N, os.cpu_count())}
-            Tg, Wg = Tx[0].cpu().numpy(), Wx[0].cpu().numpy()
             line["parity"] = {
                 "Wx_rel_l2": float(np.linalg.norm(Wg - Wo) / np.linalg.norm(Wo)),
                 "Tx_rel_l2": float(np.linalg.norm(Tg - To) / np.linalg.norm(To))}
@@ -329,6 +420,10 @@ def main():
                     help='skip the end-to-end (host buffers) leg')
     ap.add_argument('--arith', default='float64', choices=['float64', 'float32'],
                     help='arithmetic inside the transforms (data stay float32)')
+    ap.add_argument('--no-batch', action='store_true',
+                    help='skip the batched uneven-length leg')
+    ap.add_argument('--batch', type=int, default=256,
+                    help='signals in the batched leg (default 256)')
     ap.add_argument('--n', type=int, default=N_SIG,
                     help='signal length (default 160000; smaller for profiling)')
     args = ap.parse_args()

@@ -235,6 +235,50 @@ SSQB_API int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_
                                 const ssqb_sig* sigs_dev, int nsig, int precision, void* Tx,
                                 void* stream);
 
+/* ---- adjoints, for reverse-mode differentiation ----------------------------
+ * ssqueezepy has no backward pass; its only differentiable piece is torch
+ * autograd through its torch-based GPU `cwt` (_cwt.py:250-311 on torch
+ * tensors). These entry points are the transposes of the forward maps, with
+ * bins held fixed (piecewise constant). Gradients follow torch's complex
+ * convention, g = dL/dRe + i dL/dIm. precision: SSQB_F32 / SSQB_F32X (float32
+ * data and arithmetic) or SSQB_F64. accumulate != 0 adds to the output
+ * instead of overwriting it. */
+
+/* Workspace bytes of ssqb_cwt_adjoint (spectrum accumulator, real inverse
+ * and a bounded chunk of rows). */
+SSQB_API size_t ssqb_cwt_adjoint_workspace_bytes(int B, int Npad, int na, int precision);
+
+/* Gradient of x through Wx = cwt(x) (the transposed CWT: per row a forward
+ * FFT of the gradient placed at the signal's padded columns, times psih,
+ * summed over rows, one inverse FFT, then the transpose of the padding). The
+ * gradient of Wx is the sum of up to three sources, each optional:
+ *   gWx (B, na, N) complex                          direct
+ *   gTx (B, nbins, N) complex through idx           c_i gTx[idx[i, j], j]
+ *     (idx (B, na, idx_pitch) from the forward, sq_weights c (na))
+ *   gxr (B, N) real through the icwt row weights    w_i gxr[j]
+ * so a whole ssq_cwt + icwt backward needs no (na, N) buffer. Output gx
+ * (B, N) real. Geometry and wavelet as in ssqb_cwt; padtype 3 (replicate) is
+ * SSQB_EUNSUPPORTED. */
+SSQB_API int ssqb_cwt_adjoint(const void* gWx, const void* gTx, const uint16_t* idx,
+                              int idx_pitch, const double* sq_weights, int nbins,
+                              const void* gxr, const double* icwt_weights, int B, int N,
+                              int Npad, int n1, int padtype, const double* scales, int na,
+                              const ssqb_wavelet* wavelet, int precision, void* gx,
+                              int accumulate, void* workspace, size_t workspace_bytes,
+                              void* stream);
+
+/* Gradient of Wx through the squeeze, a gather through the bin index:
+ * gWx[b, i, j] = row_weights[i] * gTx[b, idx[b, i, j], j] (0 where idx is
+ * 0xFFFF). Transpose of ssqb_squeeze. */
+SSQB_API int ssqb_squeeze_adjoint(const void* gTx, const uint16_t* idx, int idx_pitch,
+                                  const double* row_weights, int B, int na, int N, int nbins,
+                                  int precision, void* gWx, int accumulate, void* stream);
+
+/* Gradient of Wx through the one-integral icwt: gWx[b, i, j] =
+ * row_weights[i] * gx[b, j] (real). Transpose of ssqb_icwt. */
+SSQB_API int ssqb_icwt_adjoint(const void* gx, const double* row_weights, int B, int na,
+                               int N, int precision, void* gWx, int accumulate, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

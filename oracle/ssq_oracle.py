@@ -331,3 +331,50 @@ def icwt(Wx, scales, scaletype, nv, Cpsi, x_mean=0., l1_norm=True):
     else:
         x = x * ((2 / Cpsi) * PI / 4)
     return x + x_mean
+
+
+#### adjoints (transposes of cwt, the squeeze and icwt) #######################
+# ssqueezepy has no backward pass; these are the transposes of the forward
+# routines above (cwt: _cwt.py:246-311; squeeze: algos.py:859-895 with bins
+# held fixed; icwt: _cwt.py:479-482), used to check the adjoint kernels.
+# Gradients follow torch's complex convention g = dL/dRe + i dL/dIm, so for
+# a real x, Re <g, cwt(x)> = <x, cwt_adjoint(g)>.
+def pad_sources(N, padtype, n1, n2):
+    """Source sample of each padded position; -1 where the padding is zero."""
+    src = pad(np.arange(1, N + 1, dtype=np.float64), padtype, n1, n2)
+    return np.rint(src).astype(np.int64) - 1
+
+
+def cwt_adjoint(g, kind, params, scales, padtype='reflect'):
+    """Gradient of x (..., N) for a gradient g (..., na, N) of Wx."""
+    g = np.asarray(g, np.complex128)
+    N = g.shape[-1]
+    Npad, n1, n2 = p2up(N)
+    gp = np.zeros(g.shape[:-1] + (Npad,), np.complex128)
+    gp[..., n1:n1 + N] = g
+    H = sfft.fft(gp, axis=-1, workers=_WORKERS)
+    P, _ = psih_bank(kind, params, scales, Npad)
+    yp = sfft.ifft((P * H).sum(axis=-2), axis=-1, workers=_WORKERS).real
+    src = pad_sources(N, padtype, n1, n2)
+    keep = src >= 0
+    yp2 = yp.reshape(-1, Npad)
+    out = np.zeros((yp2.shape[0], N))
+    for b in range(yp2.shape[0]):
+        np.add.at(out[b], src[keep], yp2[b, keep])
+    return out.reshape(g.shape[:-2] + (N,))
+
+
+def squeeze_adjoint(gT, k, use, const):
+    """Gradient of Wx (na, N) for a gradient gT (na, N) of Tx: the gather
+    const[i] * gT[k[i, j], j] where `use`, else 0."""
+    na, N = k.shape
+    const = np.broadcast_to(np.asarray(const, np.float64).ravel(), (na,))
+    cols = np.broadcast_to(np.arange(N), k.shape)
+    return np.where(use, gT[k, cols] * const[:, None], 0)
+
+
+def icwt_adjoint(gx, weights):
+    """Gradient of Wx (..., na, N) for a gradient gx (..., N) of
+    x = sum_i weights[i] Re Wx[i] (+ mean): weights[i] * gx (real)."""
+    w = np.asarray(weights, np.float64).reshape(-1, 1)
+    return (w * np.asarray(gx, np.float64)[..., None, :]).astype(np.complex128)

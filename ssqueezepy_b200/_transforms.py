@@ -15,6 +15,7 @@ import os
 import numpy as np
 import torch
 
+from . import _autograd as A
 from . import _lib as L
 from . import _params as P
 
@@ -202,7 +203,8 @@ def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
     return dict(Wx=Wx, dWx=dWx, w=w, idx=idx, ipitch=ipitch, scales=scales_np,
                 scaletype=scaletype, nv=nv, na=na, N=N, dt=dt, fs=fs,
                 wavelet=wavelet, dtype=dtype, is_2d=is_2d, dev=dev, B=B,
-                gamma=gamma, sc_d=sc_d)
+                gamma=gamma, sc_d=sc_d, Npad=Npad, n1=n1, ptype=ptype, cw=cw,
+                prec=prec)
 
 
 def cwt(x, wavelet='gmw', scales='log-piecewise', fs=None, t=None, nv=32,
@@ -218,9 +220,23 @@ def cwt(x, wavelet='gmw', scales='log-piecewise', fs=None, t=None, nv=32,
     if not isinstance(scales, str):
         nv = None
     wavelet = P.process_gmw_wavelet(wavelet, l1_norm)
-    r = _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
-                  derivative)
-    Wx, dWx = r['Wx'], r['dWx']
+
+    def run(xin):
+        return _cwt_core(xin, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
+                         derivative)
+    if A.needs_grad(x):
+        _grad_checks(astensor, rpadded and padtype is not None, padtype)
+        holder = {}
+
+        def run_keep(xin):
+            holder['r'] = run(xin)
+            return holder['r']
+        outs = A.CwtFn.apply(x, run_keep)
+        r = holder['r']
+        Wx, dWx = (outs if derivative else (outs, None))
+    else:
+        r = run(x)
+        Wx, dWx = r['Wx'], r['dWx']
     if not l1_norm:
         s = torch.as_tensor(np.sqrt(r['scales'].ravel()), device=r['dev'],
                             dtype=_RDT[r['dtype']]).reshape(1, -1, 1)
@@ -229,6 +245,17 @@ def cwt(x, wavelet='gmw', scales='log-piecewise', fs=None, t=None, nv=32,
     scales_out = _scales_out(r, astensor)
     Wx, dWx = _out(Wx, astensor, r['is_2d']), _out(dWx, astensor, r['is_2d'])
     return (Wx, scales_out, dWx) if derivative else (Wx, scales_out)
+
+
+def _grad_checks(astensor, rpadded, padtype):
+    if not astensor:
+        raise ValueError("differentiable transforms return tensors: use astensor=True")
+    if rpadded:
+        raise NotImplementedError("gradients of `rpadded=True` outputs are not "
+                                  "implemented")
+    if padtype == 'replicate':
+        raise NotImplementedError("gradients through padtype='replicate' are not "
+                                  "implemented")
 
 
 def _scales_out(r, astensor):
@@ -329,18 +356,33 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
 
     fp = _ssq_plan(wavelet, scales, N, nv, ssq_freqs, maprange, padtype, dt, sp)
     f_asc = fp['f_asc']
-    r = _cwt_core(x, wavelet, scales, nv, fs, t, padtype, False, nan_checks,
-                  get_dWx, want_idx=True, want_w=get_w,
-                  ssq=(fp['mode'], fp['bp'], na, flipud), gamma=gamma)
-    Tx = torch.empty_like(r['Wx'])
-    cst = _on_device(fp, 'const', r['dev'])
-    with torch.cuda.device(r['dev']):
-        rc = L.load().ssqb_squeeze(L.ptr(r['Wx']), L.ptr(r['idx']), r['ipitch'],
-                                   L.ptr(cst), r['B'], na, N, na, _prec(r['dtype']),
-                                   L.ptr(Tx), L.stream_ptr())
-    L.check(rc, 'squeeze')
+    def run(xin):
+        r = _cwt_core(xin, wavelet, scales, nv, fs, t, padtype, False, nan_checks,
+                      get_dWx, want_idx=True, want_w=get_w,
+                      ssq=(fp['mode'], fp['bp'], na, flipud), gamma=gamma)
+        Tx = torch.empty_like(r['Wx'])
+        cst = _on_device(fp, 'const', r['dev'])
+        with torch.cuda.device(r['dev']):
+            rc = L.load().ssqb_squeeze(L.ptr(r['Wx']), L.ptr(r['idx']), r['ipitch'],
+                                       L.ptr(cst), r['B'], na, N, na, _prec(r['dtype']),
+                                       L.ptr(Tx), L.stream_ptr())
+        L.check(rc, 'squeeze')
+        return Tx, r, cst
+
+    if A.needs_grad(x):
+        _grad_checks(astensor, False, padtype)
+        holder = {}
+
+        def run_keep(xin):
+            holder['out'] = run(xin)
+            return holder['out']
+        Tx, Wx = A.SsqCwtFn.apply(x, run_keep)
+        r = holder['out'][1]
+    else:
+        Tx, r, _ = run(x)
+        Wx = r['Wx']
     is2 = r['is_2d']
-    out = [_out(Tx, astensor, is2), _out(r['Wx'], astensor, is2), f_asc[::-1],
+    out = [_out(Tx, astensor, is2), _out(Wx, astensor, is2), f_asc[::-1],
            _scales_out(r, astensor)]
     if get_w:
         out.append(_out(r['w'], astensor, is2))
@@ -361,6 +403,10 @@ def icwt(Wx, wavelet='gmw', scales='log-piecewise', nv=None, one_int=True,
     if not W.is_complex():
         raise ValueError("`Wx` must be complex")
     L.require_cuda()
+    grad = A.needs_grad(W)
+    if grad and rpadded:
+        raise NotImplementedError("gradients of icwt with rpadded=True are not "
+                                  "implemented")
     W = W.to(_device_of(Wx)).contiguous()
     is3 = W.ndim == 3
     W3 = W if is3 else W[None]
@@ -370,31 +416,49 @@ def icwt(Wx, wavelet='gmw', scales='log-piecewise', nv=None, one_int=True,
         nv = 32
     wavelet = P.process_gmw_wavelet(wavelet, l1_norm)
     wavelet = P.Wavelet._init_if_not_isinstance(wavelet)
-    if isinstance(scales, str):
-        sc, st, _, nv = P.process_scales(scales, x_len, wavelet, nv=nv,
-                                         get_params=True)
-    else:
-        sc, st, _, nv = P.process_scales(P._to_numpy(scales), x_len,
-                                         get_params=True)
-    sc = np.asarray(sc, np.float64).ravel()
-    if len(sc) != na:
-        raise AssertionError("%s != %s" % (len(sc), na))
-    Cpsi = P.adm_ssq(wavelet)
-    weights, mean_mult = _icwt_weights(sc, st, Cpsi, l1_norm)
+    ip = _icwt_plan(wavelet, scales, x_len, nv, l1_norm)
+    if len(ip['weights']) != na:
+        raise AssertionError("%s != %s" % (len(ip['weights']), na))
     xm = np.broadcast_to(np.asarray(x_mean, np.float64).ravel(), (B,)) \
         if np.size(x_mean) in (1, B) else None
     if xm is None:
         raise ValueError("`x_mean` must be a scalar or have one value per input")
     prec = L.F64 if W3.dtype == torch.complex128 else L.F32
-    out = torch.empty((B, n), dtype=torch.float64 if prec else torch.float32,
-                      device=W3.device)
-    wd, xmd = _dev_f64(weights, W3.device), _dev_f64(xm, W3.device)
-    with torch.cuda.device(W3.device):
-        rc = L.load().ssqb_icwt(L.ptr(W3), L.ptr(wd), L.ptr(xmd), float(mean_mult),
-                                B, na, n, prec, L.ptr(out), L.stream_ptr())
-    L.check(rc, 'icwt')
+    wd = _on_device(ip, 'weights', W3.device)
+
+    def run(Win):
+        Win = Win.contiguous()
+        out = torch.empty((B, n), dtype=torch.float64 if prec else torch.float32,
+                          device=Win.device)
+        xmd = _dev_f64(xm, Win.device)
+        with torch.cuda.device(Win.device):
+            rc = L.load().ssqb_icwt(L.ptr(Win), L.ptr(wd), L.ptr(xmd),
+                                    float(ip['mean_mult']), B, na, n, prec, L.ptr(out),
+                                    L.stream_ptr())
+        L.check(rc, 'icwt')
+        return out, wd
+
+    if grad:
+        out = A.IcwtFn.apply(W3, run)
+    else:
+        out, _ = run(W3)
     out = out if is3 else out[0]
     return out.cpu().numpy() if is_np else out
+
+
+def _icwt_plan(wavelet, scales, x_len, nv, l1_norm):
+    """Row weights of the one-integral inverse (cached float64)."""
+    def make():
+        if isinstance(scales, str):
+            sc, st, _, nv_ = P.process_scales(scales, x_len, wavelet, nv=nv,
+                                              get_params=True)
+        else:
+            sc, st, _, nv_ = P.process_scales(P._to_numpy(scales), x_len,
+                                              get_params=True)
+        sc = np.asarray(sc, np.float64).ravel()
+        weights, mean_mult = _icwt_weights(sc, st, P.adm_ssq(wavelet), l1_norm)
+        return dict(weights=weights, mean_mult=mean_mult)
+    return _plan(('icwt', _wkey(wavelet), x_len, _akey(scales), nv, l1_norm), make)
 
 
 def _icwt_weights(scales, scaletype, Cpsi, l1_norm):

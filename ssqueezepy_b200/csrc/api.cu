@@ -581,4 +581,117 @@ int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_sig* sigs
   return SSQB_OK;
 }
 
+// ---- adjoints ------------------------------------------------------------------
+static int check_adj_sources(const void* gWx, const void* gTx, const uint16_t* idx,
+                             int idx_pitch, const double* sq_weights, int nbins,
+                             const void* gxr, const double* icwt_weights, int N) {
+  if (!gWx && !gTx && !gxr) return fail(SSQB_EINVAL, "no gradient source given");
+  if (gTx) {
+    if (!idx || !sq_weights) return fail(SSQB_EINVAL, "gTx needs idx and sq_weights");
+    if (nbins < 1 || nbins > 65535) return fail(SSQB_EINVAL, "nbins must be in [1, 65535]");
+    if (idx_pitch < N) return fail(SSQB_EINVAL, "idx_pitch smaller than N");
+  }
+  if (gxr && !icwt_weights) return fail(SSQB_EINVAL, "gxr needs icwt_weights");
+  return SSQB_OK;
+}
+
+size_t ssqb_cwt_adjoint_workspace_bytes(int B, int Npad, int na, int precision) {
+  if (B < 1 || na < 1 || !is_pow2(Npad) || !valid_precision(precision)) return 0;
+  return cwt_adjoint_workspace(B, Npad, na, data_prec(precision) == SSQB_F64);
+}
+
+int ssqb_cwt_adjoint(const void* gWx, const void* gTx, const uint16_t* idx, int idx_pitch,
+                     const double* sq_weights, int nbins, const void* gxr,
+                     const double* icwt_weights, int B, int N, int Npad, int n1, int padtype,
+                     const double* scales, int na, const ssqb_wavelet* wavelet, int precision,
+                     void* gx, int accumulate, void* workspace, size_t workspace_bytes,
+                     void* stream) {
+  if (!scales || !gx || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
+  if (B > 65535 || na > 65535) return fail(SSQB_EINVAL, "B and na must be <= 65535");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
+    return fail(SSQB_EUNSUPPORTED, "Npad must be a power of two in [8, 2^22]");
+  if (Npad < N || n1 < 0 || n1 + N > Npad) return fail(SSQB_EINVAL, "bad padding geometry");
+  if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
+  if (padtype == 3)
+    return fail(SSQB_EUNSUPPORTED, "the adjoint of replicate padding is not implemented");
+  if (idx_pitch == 0) idx_pitch = N;
+  int r = check_adj_sources(gWx, gTx, idx, idx_pitch, sq_weights, nbins, gxr, icwt_weights, N);
+  if (r) return r;
+  WavDev wd;
+  r = check_wavelet(wavelet, &wd);
+  if (r) return r;
+  const bool f64 = data_prec(precision) == SSQB_F64;
+  const size_t need = cwt_adjoint_workspace(B, Npad, 1, f64);
+  if (workspace_bytes < need)
+    return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                     " bytes");
+  Tables tb;
+  r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  int e;
+  if (f64) {
+    AdjSources<double2> src{(const double2*)gWx, (const double2*)gTx, idx, idx_pitch, nbins,
+                            sq_weights, (const double*)gxr, icwt_weights};
+    e = run_cwt_adjoint_f64(src, B, N, Npad, n1, padtype, scales, na, wd, (double*)gx,
+                            accumulate, workspace, workspace_bytes, tb, st);
+  } else {
+    AdjSources<float2> src{(const float2*)gWx, (const float2*)gTx, idx, idx_pitch, nbins,
+                           sq_weights, (const float*)gxr, icwt_weights};
+    e = run_cwt_adjoint_f32(src, B, N, Npad, n1, padtype, scales, na, wd, (float*)gx,
+                            accumulate, workspace, workspace_bytes, tb, st);
+  }
+  if (e) return cuda_fail((cudaError_t)e, "cwt adjoint launch");
+  return SSQB_OK;
+}
+
+static int wx_adjoint(const void* gTx, const uint16_t* idx, int idx_pitch,
+                      const double* sq_weights, int nbins, const void* gxr,
+                      const double* icwt_weights, int B, int na, int N, int precision,
+                      void* gWx, int accumulate, void* stream) {
+  if (!gWx) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
+  if (B > 65535 || na > 65535) return fail(SSQB_EINVAL, "B and na must be <= 65535");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  if (idx_pitch == 0) idx_pitch = N;
+  int r = check_adj_sources(nullptr, gTx, idx, idx_pitch, sq_weights, nbins, gxr,
+                            icwt_weights, N);
+  if (r) return r;
+  Tables tb;
+  r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  int e;
+  if (data_prec(precision) == SSQB_F64) {
+    AdjSources<double2> src{nullptr, (const double2*)gTx, idx, idx_pitch, nbins, sq_weights,
+                            (const double*)gxr, icwt_weights};
+    e = run_wx_adjoint_f64(src, B, na, N, (double2*)gWx, accumulate, tb.status, st);
+  } else {
+    AdjSources<float2> src{nullptr, (const float2*)gTx, idx, idx_pitch, nbins, sq_weights,
+                           (const float*)gxr, icwt_weights};
+    e = run_wx_adjoint_f32(src, B, na, N, (float2*)gWx, accumulate, tb.status, st);
+  }
+  if (e) return cuda_fail((cudaError_t)e, "adjoint launch");
+  return SSQB_OK;
+}
+
+int ssqb_squeeze_adjoint(const void* gTx, const uint16_t* idx, int idx_pitch,
+                         const double* row_weights, int B, int na, int N, int nbins,
+                         int precision, void* gWx, int accumulate, void* stream) {
+  if (!gTx) return fail(SSQB_EINVAL, "NULL pointer argument");
+  return wx_adjoint(gTx, idx, idx_pitch, row_weights, nbins, nullptr, nullptr, B, na, N,
+                    precision, gWx, accumulate, stream);
+}
+
+int ssqb_icwt_adjoint(const void* gx, const double* row_weights, int B, int na, int N,
+                      int precision, void* gWx, int accumulate, void* stream) {
+  if (!gx) return fail(SSQB_EINVAL, "NULL pointer argument");
+  return wx_adjoint(nullptr, nullptr, 0, nullptr, 0, gx, row_weights, B, na, N, precision,
+                    gWx, accumulate, stream);
+}
+
 }  // extern "C"

@@ -88,4 +88,20 @@ int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* 
                           int nsig, int max_na, int max_N, float2* Tx, int* status,
                           cudaStream_t st);
 
+// adjoints (reverse-mode differentiation)
+constexpr size_t kAdjChunkBytes = (size_t)64 << 20;  // row chunk: Y + Z
+size_t cwt_adjoint_workspace(int B, int Npad, int na, bool f64);
+int run_cwt_adjoint_f32(const AdjSources<float2>& src, int B, int N, int Npad, int n1,
+                        int padtype, const double* scales, int na, const WavDev& wd, float* gx,
+                        int accumulate, void* ws, size_t ws_bytes, const Tables& tb,
+                        cudaStream_t st);
+int run_cwt_adjoint_f64(const AdjSources<double2>& src, int B, int N, int Npad, int n1,
+                        int padtype, const double* scales, int na, const WavDev& wd,
+                        double* gx, int accumulate, void* ws, size_t ws_bytes,
+                        const Tables& tb, cudaStream_t st);
+int run_wx_adjoint_f32(const AdjSources<float2>& src, int B, int na, int N, float2* gWx,
+                       int accumulate, int* status, cudaStream_t st);
+int run_wx_adjoint_f64(const AdjSources<double2>& src, int B, int na, int N, double2* gWx,
+                       int accumulate, int* status, cudaStream_t st);
+
 }  // namespace ssqb

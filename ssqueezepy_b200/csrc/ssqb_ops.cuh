@@ -394,4 +394,40 @@ struct CwtBatchOp {
   }
 };
 
+// ---- gradient of Wx for the adjoints ----------------------------------------
+// Gradient of Wx at (signal b, row i, column j): the sum of the supplied
+// sources (any may be absent): the direct gradient, the squeeze's gather
+// c_i gTx[idx[i, j], j] and the icwt's w_i gx[j].
+template <typename C>
+struct AdjSources {
+  typedef typename RealOf<C>::type T;
+  const C* gW;              // (B, na, N) gradient of Wx
+  const C* gT;              // (B, nbins, N) gradient of Tx
+  const uint16_t* idx;      // (B, na, idx_pitch) bins of the forward
+  int idx_pitch, nbins;
+  const double* sqw;        // (na) squeeze weights
+  const T* gxr;             // (B, N) gradient of the icwt output
+  const double* icw;        // (na) icwt row weights
+  __device__ __forceinline__ C at(int b, int na, int N, int i, int j, int* status) const {
+    C acc = mk((T)0, (T)0);
+    const size_t o = ((size_t)b * na + i) * N + j;
+    if (gW) acc = gW[o];
+    if (gT) {
+      const uint16_t k = idx[((size_t)b * na + i) * idx_pitch + j];
+      if (k != kNoBin) {
+        if (k < nbins) {
+          const C t = gT[((size_t)b * nbins + k) * N + j];
+          const T c = (T)sqw[i];
+          acc.x += t.x * c;
+          acc.y += t.y * c;
+        } else {
+          set_status(status, DEV_BAD_BIN);
+        }
+      }
+    }
+    if (gxr) acc.x += gxr[(size_t)b * N + j] * (T)icw[i];
+    return acc;
+  }
+};
+
 }  // namespace ssqb

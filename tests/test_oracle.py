@@ -98,3 +98,36 @@ def test_oracle_full_size_digest_10k(golden_digests):
     assert np.allclose(Tx[r][::16], d['d10k/Tx_row'], rtol=1e-9, atol=1e-12)
     fin = np.isfinite(w)
     assert fin.sum() == int(d['d10k/w_finite'])
+
+
+@pytest.mark.parametrize('padtype', ['reflect', 'zero', 'symmetric', 'wrap'])
+@pytest.mark.parametrize('N', [300, 1000])
+def test_cwt_adjoint_is_the_transpose(padtype, N):
+    """Re <g, cwt(x)> == <x, cwt_adjoint(g)> (the dot-product test), float64."""
+    rng = np.random.default_rng(N)
+    scales = np.geomspace(1.5, N / 8, 40)
+    x = rng.standard_normal((2, N))
+    g = rng.standard_normal((2, 40, N)) + 1j * rng.standard_normal((2, 40, N))
+    Wx, _ = O.cwt(x, 'morlet', (6.,), scales, padtype=padtype, derivative=False)
+    gx = O.cwt_adjoint(g, 'morlet', (6.,), scales, padtype=padtype)
+    lhs = np.real(np.vdot(g, Wx))
+    rhs = float(np.sum(x * gx))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+def test_squeeze_and_icwt_adjoints_are_transposes():
+    rng = np.random.default_rng(5)
+    na, N = 30, 200
+    W = rng.standard_normal((na, N)) + 1j * rng.standard_normal((na, N))
+    k = rng.integers(0, na, (na, N))
+    use = rng.random((na, N)) > 0.2
+    c = rng.random(na)
+    gT = rng.standard_normal((na, N)) + 1j * rng.standard_normal((na, N))
+    T = O.squeeze(W, k, use, c)
+    gW = O.squeeze_adjoint(gT, k, use, c)
+    assert abs(np.real(np.vdot(gT, T)) - np.real(np.vdot(gW, W))) < 1e-10 * np.abs(T).sum()
+    w = rng.random(na)
+    gx = rng.standard_normal(N)
+    xr = (w[:, None] * W.real).sum(0)
+    gW2 = O.icwt_adjoint(gx, w)
+    assert abs(float(gx @ xr) - np.real(np.vdot(gW2, W))) < 1e-10 * np.abs(xr).sum()
