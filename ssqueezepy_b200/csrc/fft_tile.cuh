@@ -14,6 +14,7 @@
 // padded to a stride chosen so that both row-fastest and column-fastest
 // thread mappings hit distinct banks.
 #pragma once
+#include <type_traits>
 #include "ssqb_common.cuh"
 
 namespace ssqb {
@@ -145,6 +146,13 @@ template <> __device__ __forceinline__ const double2* seg_table<double2>(const T
   return t.seg_d;
 }
 
+// A loader with `kGather` gathers the R inputs of one first-stage item at
+// once (`gather<R>(f, j, stride, t)`: inputs j + r*stride of row f), so that
+// it can issue all of its memory loads before the arithmetic on them.
+template <class T, class = void> struct HasGather : std::false_type {};
+template <class T>
+struct HasGather<T, std::void_t<decltype(T::kGather)>> : std::bool_constant<T::kGather> {};
+
 // One full transform of the tile.
 //   ld(f, m, C (&v)[NARR])   input element m of row f (all arrays)
 //   st.item<R>(f, m0, stride, C (&a)[R], C (&b)[R])
@@ -180,14 +188,22 @@ __device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __rest
     if (NB % NT == 0 || it < NB) {
       int f, j;
       item_fj<MAP, NF, LR>(it, f, j);
+      if constexpr (FIRST && HasGather<LD>::value) {
+        C t[R][NARR];
+        ld.template gather<R>(f, j, L / R, t);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+          for (int a = 0; a < NARR; ++a) v[a][p][r] = t[r][a];
+      }
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        if constexpr (FIRST) {
+        if constexpr (FIRST && !HasGather<LD>::value) {
           C t[NARR];
           ld(f, j + r * (L / R), t);
 #pragma unroll
           for (int a = 0; a < NARR; ++a) v[a][p][r] = t[a];
-        } else {
+        } else if constexpr (!FIRST) {
 #pragma unroll
           for (int a = 0; a < NARR; ++a) v[a][p][r] = buf[a][LY::at(f, j + r * (L / R))];
         }

@@ -266,12 +266,33 @@ struct CwtOp {
   int* status;
   __device__ CwtOp bind(int) const { return *this; }
   __device__ int rows() const { return na; }
+  // Split load (spectrum value first, then the wavelet), and the signed bin
+  // range [klo, khi] outside which psih(scale * xi) is exactly 0 (one bin of
+  // margin each side; psih still applies its own band test inside).
+  static constexpr bool kSplitLoad = true;
+  __device__ void band_bins(int row, int& klo, int& khi) const {
+    klo = -Npad;
+    khi = Npad;
+    if (wav.lo < wav.hi) {
+      const double sh = scales[row] * h;
+      const double a = floor(wav.lo / sh) - 1.0, c = ceil(wav.hi / sh) + 1.0;
+      klo = (int)fmax(fmin(a, (double)Npad), -(double)Npad);
+      khi = (int)fmax(fmin(c, (double)Npad), -(double)Npad);
+    }
+  }
+  __device__ double2 raw(int b, int k, int klo, int khi) const {
+    const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
+    return (kk >= klo && kk <= khi) ? __ldg(xh + (size_t)b * Npad + k)
+                                    : make_double2(0.0, 0.0);
+  }
   __device__ void load(int b, int row, int k, C (&v)[2]) const {
+    finish(b, row, k, __ldg(xh + (size_t)b * Npad + k), v);
+  }
+  __device__ void finish(int, int row, int k, double2 xv, C (&v)[2]) const {
     const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
     const double xi = (double)kk * h;
     double ps = psih_fp64(wav, scales[row] * xi);
     if (k == (Npad >> 1)) ps *= 0.5;  // Nyquist bin halved (wavelets.py:86-95)
-    const double2 xv = __ldg(xh + (size_t)b * Npad + k);
     const double2 y = make_double2(ps * xv.x, ps * xv.y);
     const double c = xi * inv_dt;
     v[0] = to_c<C>(y);

@@ -84,6 +84,47 @@ struct Pass1Store {
   }
 };
 
+// Pass-1 loader: input k1_0 + f + L1*m of row `row`. Ops with a split load
+// get a gather that issues the R spectrum loads of an item (only those in
+// the row's wavelet band) before any wavelet arithmetic.
+template <class BOp, typename C, int NARR, class = void>
+struct P1Loader {
+  const BOp& op;
+  int b, row, k1_0, L1;
+  __device__ __forceinline__ void operator()(int f, int m, C (&v)[NARR]) const {
+    op.load(b, row, k1_0 + f + L1 * m, v);
+  }
+};
+template <class BOp, typename C, int NARR>
+struct P1Loader<BOp, C, NARR, std::enable_if_t<BOp::kSplitLoad>> {
+  static constexpr bool kGather = true;
+  const BOp& op;
+  int b, row, k1_0, L1, klo, khi;
+  __device__ __forceinline__ void operator()(int f, int m, C (&v)[NARR]) const {
+    op.load(b, row, k1_0 + f + L1 * m, v);
+  }
+  template <int R>
+  __device__ __forceinline__ void gather(int f, int j, int stride, C (&t)[R][NARR]) const {
+    double2 raw[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) raw[r] = op.raw(b, k1_0 + f + L1 * (j + r * stride), klo, khi);
+#pragma unroll
+    for (int r = 0; r < R; ++r) op.finish(b, row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
+  }
+};
+
+template <class BOp, typename C, int NARR>
+__device__ __forceinline__ P1Loader<BOp, C, NARR> make_p1_loader(const BOp& op, int b, int row,
+                                                                  int k1_0, int L1) {
+  if constexpr (HasGather<P1Loader<BOp, C, NARR>>::value) {
+    int klo, khi;
+    op.band_bins(row, klo, khi);
+    return P1Loader<BOp, C, NARR>{op, b, row, k1_0, L1, klo, khi};
+  } else {
+    return P1Loader<BOp, C, NARR>{op, b, row, k1_0, L1};
+  }
+}
+
 template <class Op, typename C, int LOGL, int SIGN>
 __global__ void __launch_bounds__(kNT, MinBlocks<C>::v)
 tile_single(Op op, Tables tb) {
@@ -150,7 +191,8 @@ tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_
   const int k1_0 = blockIdx.x * NF;
   const size_t L = size_t(1) << log2L;
   C* zrow = Z + (size_t(blockIdx.z) * rows_in_tile + blockIdx.y) * NARR * L;
-  auto ld = [&](int f, int m, C (&v)[NARR]) { bop.load(b, row, k1_0 + f + L1 * m, v); };
+  typedef decltype(op.bind(0)) BOp;
+  const auto ld = make_p1_loader<BOp, C, NARR>(bop, b, row, k1_0, L1);
   Pass1Store<C, NARR, SIGN> st{tb, zrow, k1_0, L1, log2L};
   fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
