@@ -1,19 +1,28 @@
 # -*- coding: utf-8 -*-
-"""Benchmark of the synchrosqueezing hot path: ssq_cwt forward, float32,
-one N=160,000 signal per GPU per step (linear chirp 0.01->0.2 cycles/sample +
-AM tone at 0.3 + N(0, 0.1^2) noise), GMW gamma=3 beta=60, nv=32,
-log-piecewise scales (293 rows), reflect padding (Npad = 262,144).
+"""Benchmark of the synchrosqueezing hot path on one B200 per rank.
+
+Headline (the JSON line's `value`): ssq_cwt forward, float32, one N=160,000
+signal per GPU per step (linear chirp 0.01->0.2 cycles/sample + AM tone at
+0.3 + N(0, 0.1^2) noise), GMW gamma=3 beta=60, nv=32, log-piecewise scales
+(293 rows), reflect padding (Npad = 262,144), inputs resident in HBM and
+outputs preallocated (the C-ABI calls of one ssq_cwt: fused CWT + squeeze).
+`e2e` is the same metric through the public `ssq_cwt` call from pinned host
+memory, with the host->device copy of x and the device->host copy of Tx.
+
+Further legs, each a key of the same line:
+  batched  256 signals of uneven length in [4096, 65536], Morlet mu=6, one
+           SsqCwtBatch plan (CUDA graph) vs one ssq_cwt call per signal;
+  long     8 x N=1,048,576, GMW, 'log:maximal' (613 rows): plain forward,
+           batched forward, forward + backward, peak memory;
+  fwd_bwd  64 x N=16,384 Morlet: loss MSE(|Tx(x)|,|Tx(y)|) + MSE(icwt(Wx), y),
+           forward vs forward + backward through the adjoint kernels.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line (rank 0). `value` is signal-samples/s over all ranks with
-inputs resident in HBM and outputs preallocated (the C-ABI calls of one
-ssq_cwt: fused CWT + squeeze); `e2e` is the same metric through the public
-`ssq_cwt` call from pinned host memory, including the host->device copy of x
-and the device->host copy of Tx. Each rank processes its own signal (weak
-scaling, no collective on the data path). `--impl reference` times the CPU
-restatement of ssqueezepy's algorithm (oracle/ssq_oracle.py, float64, all
-host threads) on the same workload.
+Each rank processes its own signals (weak scaling, no collective on the
+data path). `--impl reference` times the CPU restatement of ssqueezepy's
+algorithm (oracle/ssq_oracle.py, float64, all host threads) on the headline
+workload.
 """
 import argparse
 import json
@@ -242,10 +251,18 @@ def run_ours(args):
     if not args.no_batch:
         del Wx, Tx, idx, ws
         batched = run_batched(args, torch, dev, world, barrier, flush)
+    long_ = None
+    if not args.no_long:
+        torch.cuda.empty_cache()
+        long_ = run_long(args, torch, dev, world, barrier)
+    train = None
+    if not args.no_train:
+        torch.cuda.empty_cache()
+        train = run_train(args, torch, dev, world, barrier, flush)
     clocks = clk.stop() if clk else None
     if rank == 0:
         emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
-             launches, clocks, sc, f, const, Tx_keep, Wx_keep, batched)
+             launches, clocks, sc, f, const, Tx_keep, Wx_keep, batched, train, long_)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -358,8 +375,156 @@ def run_batched(args, torch, dev, world, barrier, flush):
     }
 
 
+def run_train(args, torch, dev, world, barrier, flush):
+    """Differentiable ssq_cwt + icwt on a batch of 64 float32 signals of
+    N = 16,384 (chirp mixtures), Morlet mu=6, nv=32 log-piecewise: loss =
+    MSE(|Tx(x)|, |Tx(y)|) + MSE(icwt(Wx(x)), y). Times the forward (loss)
+    and forward + backward (gradient of x through the adjoint kernels)."""
+    import torch.distributed as dist
+    import ssqueezepy_b200 as sb
+    from ssqueezepy_b200 import _signals as S
+    rank = int(os.environ.get('RANK', 0))
+    B, N = args.train_batch, 16384
+    wav = ('morlet', {'mu': 6., 'dtype': 'float32'})
+    xs = torch.tensor(S.same_length_batch(B, N, 5678 + rank), dtype=torch.float32,
+                      device=dev)
+    y = torch.tensor(S.same_length_batch(B, N, 9012 + rank), dtype=torch.float32,
+                     device=dev)
+    with torch.no_grad():
+        Ty = sb.ssq_cwt(y, wav)[0].abs()
+
+    def fwd(x):
+        Tx, Wx, _, _ = sb.ssq_cwt(x, wav)
+        xr = sb.icwt(Wx, wav, x_len=N)
+        return ((Tx.abs() - Ty) ** 2).mean() + ((xr - y) ** 2).mean()
+
+    x = xs.clone().requires_grad_(True)
+    st = torch.cuda.current_stream()
+    for _ in range(max(args.warmup, 3)):
+        fwd(x).backward()
+    barrier()
+    steps = max(1, min(args.steps, 5))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    flush.zero_()
+    ev[0].record(st)
+    for _ in range(steps):
+        with torch.no_grad():
+            fwd(xs)
+    ev[1].record(st)
+    barrier()
+    flush.zero_()
+    ev[2].record(st)
+    for _ in range(steps):
+        x.grad = None
+        fwd(x).backward()
+    ev[3].record(st)
+    barrier()
+    t = torch.tensor([ev[0].elapsed_time(ev[1]) / steps, ev[2].elapsed_time(ev[3]) / steps],
+                     dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    f_ms, fb_ms = float(t[0]), float(t[1])
+    peak = torch.cuda.max_memory_allocated(dev)
+    return {
+        "workload": "ssq_cwt + icwt loss, batch %d x N=%d float32 chirp mixtures, "
+                    "Morlet mu=6 nv=32 log-piecewise; backward through the adjoint "
+                    "kernels (bins held fixed)" % (B, N),
+        "fwd_value": world * B * N / (f_ms * 1e-3), "fwd_ms": f_ms,
+        "fwd_bwd_value": world * B * N / (fb_ms * 1e-3), "fwd_bwd_ms": fb_ms,
+        "fwd_bwd_over_fwd": fb_ms / f_ms, "unit": UNIT,
+        "peak_memory_gb": peak / 1e9,
+    }
+
+
+def run_long(args, torch, dev, world, barrier):
+    """Long signals: 8 float32 chirp mixtures of N = 1,048,576 (Npad 2,097,152),
+    GMW(3,60), scales='log:maximal' (613 rows). Plain forward (one signal per
+    call), batched forward (all 8 in one call) and forward + backward of
+    MSE(|Tx(x)|, |Tx(y)|) + MSE(icwt(Wx(x)), y) one signal at a time. The
+    backward keeps only the uint16 bin index of the forward (not Wx) and
+    needs no recomputation of Wx."""
+    import torch.distributed as dist
+    import ssqueezepy_b200 as sb
+    from ssqueezepy_b200 import _signals as S
+    rank = int(os.environ.get('RANK', 0))
+    B, N = 8, 1 << 20
+    wav = ('gmw', {'gamma': 3., 'beta': 60., 'dtype': 'float32'})
+    kw = dict(scales='log:maximal')
+    xs = torch.tensor(S.same_length_batch(B, N, 4321 + rank), dtype=torch.float32,
+                      device=dev)
+    ys = torch.tensor(S.same_length_batch(B, N, 8765 + rank), dtype=torch.float32,
+                      device=dev)
+    st = torch.cuda.current_stream()
+    steps = max(1, min(args.steps, 2))
+
+    def timed(fn, n):
+        fn()
+        barrier()
+        torch.cuda.reset_peak_memory_stats(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(n):
+            fn()
+        e1.record(st)
+        barrier()
+        return e0.elapsed_time(e1) / n, torch.cuda.max_memory_allocated(dev) / 1e9
+
+    na = int(sb.ssq_cwt(xs[0], wav, **kw)[1].shape[0])
+
+    def plain():
+        for i in range(B):
+            sb.ssq_cwt(xs[i], wav, **kw)
+
+    def batched():
+        sb.ssq_cwt(xs, wav, **kw)
+
+    with torch.no_grad():
+        Ty = [sb.ssq_cwt(ys[i], wav, **kw)[0].abs() for i in range(B)]
+
+    def fwd_bwd():
+        for i in range(B):
+            x = xs[i].clone().requires_grad_(True)
+            Tx, Wx, _, _ = sb.ssq_cwt(x, wav, **kw)
+            xr = sb.icwt(Wx, wav, x_len=N, **kw)
+            del Wx
+            loss = ((Tx.abs() - Ty[i]) ** 2).mean() + ((xr - ys[i]) ** 2).mean()
+            del Tx, xr
+            loss.backward()
+
+    with torch.no_grad():
+        p_ms, p_mem = timed(plain, steps)
+        torch.cuda.empty_cache()
+        b_ms, b_mem = timed(batched, steps)
+    torch.cuda.empty_cache()
+    fb_ms, fb_mem = timed(fwd_bwd, steps)
+    del Ty
+    torch.cuda.empty_cache()
+    t = torch.tensor([p_ms, b_ms, fb_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    p_ms, b_ms, fb_ms = (float(v) for v in t)
+    hbm, src = peaks()
+    fwd_bytes = B * N * (4 + 16 * na)
+    bwd_bytes = B * N * (8 * na + 4 + 4)
+    frac = lambda by, ms: by / (ms * 1e-3) / 1e9 / hbm
+    return {
+        "workload": "ssq_cwt, %d float32 chirp mixtures of N = %d, GMW(3,60), "
+                    "scales='log:maximal' (%d rows), reflect" % (B, N, na),
+        "plain_fwd": {"value": world * B * N / (p_ms * 1e-3), "ms": p_ms,
+                      "hbm_frac": frac(fwd_bytes, p_ms), "peak_memory_gb": p_mem},
+        "batched_fwd": {"value": world * B * N / (b_ms * 1e-3), "ms": b_ms,
+                        "hbm_frac": frac(fwd_bytes, b_ms), "peak_memory_gb": b_mem},
+        "fwd_bwd": {"value": world * B * N / (fb_ms * 1e-3), "ms": fb_ms,
+                    "hbm_frac": frac(fwd_bytes + bwd_bytes, fb_ms),
+                    "peak_memory_gb": fb_mem,
+                    "note": "one signal per forward + backward; the backward keeps the "
+                            "bin index, not Wx"},
+        "unit": UNIT, "peak_source": src,
+    }
+
+
 def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
-         launches, clocks, sc, f, const, Tg, Wg, batched=None):
+         launches, clocks, sc, f, const, Tg, Wg, batched=None, train=None, long_=None):
     hbm, src = peaks()
     if True:
         alg_cwt = (4 + 8 * na) * N          # read x, write Wx
@@ -394,6 +559,10 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
         }
         if batched is not None:
             line["batched"] = batched
+        if train is not None:
+            line["fwd_bwd"] = train
+        if long_ is not None:
+            line["long"] = long_
         if world == 1 and not args.no_cpu:
             t0 = time.perf_counter()
             To, Wo, _ = oracle_step(chirp_signal(N, seed=0), sc, f, const)
@@ -424,6 +593,12 @@ def main():
                     help='skip the batched uneven-length leg')
     ap.add_argument('--batch', type=int, default=256,
                     help='signals in the batched leg (default 256)')
+    ap.add_argument('--no-long', action='store_true',
+                    help='skip the 8 x 1,048,576 long-signal leg')
+    ap.add_argument('--no-train', action='store_true',
+                    help='skip the forward + backward (training loss) leg')
+    ap.add_argument('--train-batch', type=int, default=64,
+                    help='signals of N=16384 in the forward + backward leg')
     ap.add_argument('--n', type=int, default=N_SIG,
                     help='signal length (default 160000; smaller for profiling)')
     args = ap.parse_args()

@@ -85,11 +85,16 @@ __device__ __forceinline__ int pad_src(long long q, int N, int padtype) {
 __device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
   if (w.lo < w.hi && (x < w.lo || x > w.hi)) return 0.0;
   if (w.kind == 0) {
+    // C1 (ea - ks ec), ea = exp(-(x-mu)^2/2), ec = exp(-x^2/2). The ratio of
+    // the two terms is ks ec / ea = exp(-mu x): where mu |x| >= 40 the
+    // smaller one is below 2^-57 of the larger, under a quarter ulp, and
+    // the difference rounds to the larger term alone, so its exp is skipped.
+    const double mx = w.p0 * x;
     const double d = x - w.p0;
     const double a = -0.5 * (d * d);
     const double c = -0.5 * (x * x);
-    const double ea = a > -708.0 ? exp(a) : 0.0;
-    const double ec = c > -708.0 ? exp(c) : 0.0;
+    const double ea = (a > -708.0 && mx > -40.0) ? exp(a) : 0.0;
+    const double ec = (c > -708.0 && mx < 40.0) ? exp(c) : 0.0;
     return w.p2 * (ea - w.p1 * ec);
   }
   if (x <= 0.0) return 0.0;
