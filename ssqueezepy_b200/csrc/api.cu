@@ -224,7 +224,7 @@ size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
   size_t z = min_z_bytes(B, Npad, precision);
   if (cwt_two_pass(ilog2i(Npad), precision)) {
     const size_t per_row = (size_t)B * 2 * Npad * csize(precision);
-    size_t rows = ((size_t)48 << 20) / per_row;
+    size_t rows = kZBudgetBytes / per_row;
     if (rows < 1) rows = 1;
     if (rows > (size_t)na) rows = na;
     z = rows * per_row;
@@ -235,15 +235,31 @@ size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
 }
 
 int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_bytes) {
-  if (B < 1 || na < 1 || !is_pow2(Npad)) return -1;
-  const int m = ilog2i(Npad);
-  const int nx = two_pass<double2>(m) ? 2 : 1;
-  if (!cwt_two_pass(m, precision)) return nx + 1;
+  if (B < 1 || na < 1 || !is_pow2(Npad) || Npad < 8 || Npad > (1 << 22)) return -1;
+  if (!valid_precision(precision)) return -1;
   const size_t xb = xhat_bytes(B, Npad);
-  if (workspace_bytes < xb) return -1;
-  const size_t zcap = (workspace_bytes - xb) / csize(precision);
-  const int S = rows_per_tile(zcap, B, 2, m, na);
-  return nx + 2 * ((na + S - 1) / S);
+  if (workspace_bytes < xb + min_z_bytes(B, Npad, precision)) return -1;
+  const size_t zbytes = workspace_bytes - xb;
+  const int m = ilog2i(Npad);
+  Tables tb{};
+  int count = 0;
+  set_launch_counter(&count);
+  run_xhat_f32(nullptr, B, 1, Npad, 0, 1, nullptr, nullptr, zbytes / sizeof(double2), tb, 0);
+  if (precision == SSQB_F32) {
+    CwtOp<float2> op{};
+    op.na = na;
+    run_cwt_f32(op, B, m, nullptr, zbytes / sizeof(float2), tb, 0);
+  } else if (precision == SSQB_F32X) {
+    CwtOp<double2, float2> op{};
+    op.na = na;
+    run_cwt_f32x(op, B, m, nullptr, zbytes / sizeof(double2), tb, 0);
+  } else {
+    CwtOp<double2> op{};
+    op.na = na;
+    run_cwt_f64(op, B, m, nullptr, zbytes / sizeof(double2), tb, 0);
+  }
+  set_launch_counter(nullptr);
+  return count;
 }
 
 int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
@@ -385,6 +401,9 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
   if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
   if (!valid_precision(precision))
     return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  if (precision != SSQB_F32 && n_fft > FftCfg<double2>::TILE)
+    return fail(SSQB_EUNSUPPORTED, "n_fft above " + std::to_string(FftCfg<double2>::TILE) +
+                                       " needs float32 arithmetic");
   const int nrow = n_fft / 2 + 1;
   const int nframes = (N - 1) / hop + 1;
   if (idx_pitch == 0) idx_pitch = nframes;

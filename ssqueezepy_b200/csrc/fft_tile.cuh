@@ -23,8 +23,14 @@ template <typename C> struct FftCfg;
 template <> struct FftCfg<float2> {
   static constexpr int TILE = 4096, RMAX_LOG = 4, G_LOG = 4;
 };
+#ifndef SSQB_D_TILE
+#define SSQB_D_TILE 2048
+#endif
+#ifndef SSQB_D_RLOG
+#define SSQB_D_RLOG 3
+#endif
 template <> struct FftCfg<double2> {
-  static constexpr int TILE = 2048, RMAX_LOG = 3, G_LOG = 3;
+  static constexpr int TILE = SSQB_D_TILE, RMAX_LOG = SSQB_D_RLOG, G_LOG = 3;
 };
 
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }

@@ -9,6 +9,27 @@ static thread_local int* t_count = nullptr;
 void set_launch_counter(int* c) { t_count = c; }
 int* launch_counter() { return t_count; }
 
+AuxStream* aux_stream() {
+  static thread_local AuxStream t_aux[256];
+  static thread_local bool t_made[256], t_bad[256];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return nullptr;
+  if (t_bad[dev]) return nullptr;
+  if (!t_made[dev]) {
+    AuxStream a{};
+    if (cudaStreamCreateWithFlags(&a.s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a.join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      t_bad[dev] = true;
+      return nullptr;
+    }
+    t_aux[dev] = a;
+    t_made[dev] = true;
+  }
+  return &t_aux[dev];
+}
+
 int run_xhat_f32(const float* x, int B, int N, int Npad, int n1, int padtype,
                  double2* xh, double2* Z, size_t zcap, const Tables& tb, cudaStream_t st) {
   XhatOp<float> op{x, xh, N, Npad, n1, padtype};
@@ -23,18 +44,18 @@ int run_xhat_f64(const double* x, int B, int N, int Npad, int n1, int padtype,
 
 int run_cwt_f32(const CwtOp<float2>& op, int B, int log2L, float2* Z, size_t zcap,
                 const Tables& tb, cudaStream_t st) {
-  return run_tile<CwtOp<float2>, float2, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
+  return run_tile_signals<CwtOp<float2>, float2, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
 }
 
 int run_cwt_f64(const CwtOp<double2>& op, int B, int log2L, double2* Z, size_t zcap,
                 const Tables& tb, cudaStream_t st) {
-  return run_tile<CwtOp<double2>, double2, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
+  return run_tile_signals<CwtOp<double2>, double2, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
 }
 
 int run_cwt_f32x(const CwtOp<double2, float2>& op, int B, int log2L, double2* Z,
                  size_t zcap, const Tables& tb, cudaStream_t st) {
-  return run_tile<CwtOp<double2, float2>, double2, 1>(op, B, op.na, log2L, Z, zcap, tb,
-                                                       st);
+  return run_tile_signals<CwtOp<double2, float2>, double2, 1>(op, B, op.na, log2L, Z, zcap,
+                                                               tb, st);
 }
 
 int run_xhat_batch_f32(const float* x, const SigDesc* desc, int nsig, int Npad, int padtype,

@@ -1,5 +1,5 @@
 // Fused STFT tile kernels (one pass; power-of-two n_fft up to one tile).
-#include "launch.h"
+#include "tile_launch.cuh"
 
 namespace ssqb {
 
@@ -18,21 +18,9 @@ static int launch_stft(const Op& op, int B, const Tables& tb, cudaStream_t st) {
 
 template <class Op, typename C>
 static int run_stft(const Op& op, int B, int log2L, const Tables& tb, cudaStream_t st) {
-  switch (log2L) {
-    case 3: return launch_stft<Op, C, 3>(op, B, tb, st);
-    case 4: return launch_stft<Op, C, 4>(op, B, tb, st);
-    case 5: return launch_stft<Op, C, 5>(op, B, tb, st);
-    case 6: return launch_stft<Op, C, 6>(op, B, tb, st);
-    case 7: return launch_stft<Op, C, 7>(op, B, tb, st);
-    case 8: return launch_stft<Op, C, 8>(op, B, tb, st);
-    case 9: return launch_stft<Op, C, 9>(op, B, tb, st);
-    case 10: return launch_stft<Op, C, 10>(op, B, tb, st);
-    case 11: return launch_stft<Op, C, 11>(op, B, tb, st);
-    case 12:
-      if constexpr (tile_of<C>() >= 4096) return launch_stft<Op, C, 12>(op, B, tb, st);
-      else return (int)cudaErrorInvalidValue;
-    default: return (int)cudaErrorInvalidValue;
-  }
+  return dispatch_log<3, tile_log<C>()>(log2L, [&](auto k) {
+    return launch_stft<Op, C, decltype(k)::value>(op, B, tb, st);
+  });
 }
 
 int run_stft_f32(const StftOp<float, float2>& op, int B, int log2L, const Tables& tb,

@@ -32,6 +32,26 @@ inline int rows_per_tile(size_t zcap_elems, int B, int narr, int log2L, int nrow
   return (int)s;
 }
 
+// Budget of the two-pass intermediate of one ssqb_cwt call, bytes (kept
+// within the 126 MB L2 together with the spectrum and the streaming outputs).
+#ifndef SSQB_Z_MB
+#define SSQB_Z_MB 64
+#endif
+constexpr size_t kZBudgetBytes = (size_t)SSQB_Z_MB << 20;
+
+// Row tiles of one transform alternate between the caller's stream and an
+// auxiliary stream of this host thread (fork and join through events), each
+// with its own half of the intermediate, so that one tile's last wave
+// overlaps the next tile's first.
+#ifndef SSQB_DUAL_STREAM
+#define SSQB_DUAL_STREAM 1
+#endif
+struct AuxStream {
+  cudaStream_t s;
+  cudaEvent_t fork, join;
+};
+AuxStream* aux_stream();  // NULL if it cannot be created
+
 // single pass when L fits one tile (4096 float2 / 2048 double2 elements);
 // else two passes with log2(L2) = m/2
 template <typename C> inline bool two_pass(int log2L) {

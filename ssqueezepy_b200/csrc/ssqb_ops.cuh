@@ -271,6 +271,17 @@ struct CwtOp {
   int* status;
   __device__ CwtOp bind(int) const { return *this; }
   __device__ int rows() const { return na; }
+  // the same op for signals b0, b0+1, ... (pointers advanced by b0 signals)
+  __host__ __device__ CwtOp shifted(int b0) const {
+    CwtOp o = *this;
+    const size_t s = (size_t)b0;
+    if (o.xh) o.xh += s * Npad;
+    if (o.Wx) o.Wx += s * na * N;
+    if (o.dWx) o.dWx += s * na * N;
+    if (o.w) o.w += s * na * N;
+    if (o.idx) o.idx += s * na * idx_pitch;
+    return o;
+  }
   // Split load (spectrum value first, then the wavelet), and the signed bin
   // range [klo, khi] outside which psih(scale * xi) is exactly 0 (one bin of
   // margin each side; psih still applies its own band test inside).

@@ -2,6 +2,7 @@
 // instantiate them: one pass when L fits a tile, else two passes over row
 // tiles sized to the intermediate; batches of signals in chunks.
 #pragma once
+#include <type_traits>
 #include "launch.h"
 
 namespace ssqb {
@@ -53,26 +54,42 @@ static int launch_p2(const Op& op, int B, int log2L, const C* Z, int row_lo, int
   return cudaGetLastError();
 }
 
+// v in [LO, HI] -> f(std::integral_constant<int, v>), compile-time bounded
+template <int LO, int HI, class F>
+static int dispatch_log(int v, const F& f) {
+  if constexpr (LO > HI) {
+    return (int)cudaErrorInvalidValue;
+  } else {
+    if (v == LO) return f(std::integral_constant<int, LO>{});
+    return dispatch_log<LO + 1, HI>(v, f);
+  }
+}
+
+template <typename C> constexpr int tile_log() {
+  int m = 0;
+  while ((1 << m) < tile_of<C>()) ++m;
+  return m;
+}
+
 template <class Op, typename C, int SIGN>
 static int run_single(const Op& op, int B, int nrows, int log2L, const Tables& tb,
                       cudaStream_t st) {
-  switch (log2L) {
-    case 3: return launch_single<Op, C, SIGN, 3>(op, B, nrows, tb, st);
-    case 4: return launch_single<Op, C, SIGN, 4>(op, B, nrows, tb, st);
-    case 5: return launch_single<Op, C, SIGN, 5>(op, B, nrows, tb, st);
-    case 6: return launch_single<Op, C, SIGN, 6>(op, B, nrows, tb, st);
-    case 7: return launch_single<Op, C, SIGN, 7>(op, B, nrows, tb, st);
-    case 8: return launch_single<Op, C, SIGN, 8>(op, B, nrows, tb, st);
-    case 9: return launch_single<Op, C, SIGN, 9>(op, B, nrows, tb, st);
-    case 10: return launch_single<Op, C, SIGN, 10>(op, B, nrows, tb, st);
-    case 11: return launch_single<Op, C, SIGN, 11>(op, B, nrows, tb, st);
-    case 12:
-      if constexpr (tile_of<C>() >= 4096)
-        return launch_single<Op, C, SIGN, 12>(op, B, nrows, tb, st);
-      else
-        return (int)cudaErrorInvalidValue;
-    default: return (int)cudaErrorInvalidValue;
-  }
+  return dispatch_log<3, tile_log<C>()>(log2L, [&](auto k) {
+    return launch_single<Op, C, SIGN, decltype(k)::value>(op, B, nrows, tb, st);
+  });
+}
+
+template <class Op, typename C, int SIGN>
+static int run_rows(const Op& op, int B, int log2L, C* Z, int r0, int rows, const Tables& tb,
+                    cudaStream_t st) {
+  const int l2 = log2L / 2, l1 = log2L - l2;
+  int e = dispatch_log<3, tile_log<C>()>(l2, [&](auto k) {
+    return launch_p1<Op, C, SIGN, decltype(k)::value>(op, B, log2L, Z, r0, rows, tb, st);
+  });
+  if (e) return e;
+  return dispatch_log<3, tile_log<C>()>(l1, [&](auto k) {
+    return launch_p2<Op, C, SIGN, decltype(k)::value>(op, B, log2L, Z, r0, rows, tb, st);
+  });
 }
 
 template <class Op, typename C, int SIGN>
@@ -80,37 +97,44 @@ static int run_tile(const Op& op, int B, int nrows, int log2L, C* Z, size_t zcap
                     const Tables& tb, cudaStream_t st) {
   if (!two_pass<C>(log2L)) return run_single<Op, C, SIGN>(op, B, nrows, log2L, tb, st);
   if (log2L > 22) return (int)cudaErrorInvalidValue;
-  const int l2 = log2L / 2, l1 = log2L - l2;
   int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int S = rows_per_tile(zcap, B, Op::NARR, log2L, nrows,
-                              (1 << log2L) / tile_of<C>(), 2 * sms);
-  for (int r0 = 0; r0 < nrows; r0 += S) {
-    const int rows = (nrows - r0) < S ? (nrows - r0) : S;
-    int e;
-    switch (l2) {
-      case 6: e = launch_p1<Op, C, SIGN, 6>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 7: e = launch_p1<Op, C, SIGN, 7>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 8: e = launch_p1<Op, C, SIGN, 8>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 9: e = launch_p1<Op, C, SIGN, 9>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 10: e = launch_p1<Op, C, SIGN, 10>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 11: e = launch_p1<Op, C, SIGN, 11>(op, B, log2L, Z, r0, rows, tb, st); break;
-      default: e = (int)cudaErrorInvalidValue;
-    }
-    if (e) return e;
-    switch (l1) {
-      case 6: e = launch_p2<Op, C, SIGN, 6>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 7: e = launch_p2<Op, C, SIGN, 7>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 8: e = launch_p2<Op, C, SIGN, 8>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 9: e = launch_p2<Op, C, SIGN, 9>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 10: e = launch_p2<Op, C, SIGN, 10>(op, B, log2L, Z, r0, rows, tb, st); break;
-      case 11: e = launch_p2<Op, C, SIGN, 11>(op, B, log2L, Z, r0, rows, tb, st); break;
-      default: e = (int)cudaErrorInvalidValue;
-    }
-    if (e) return e;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
   }
-  return 0;
+  const int cpr = (1 << log2L) / tile_of<C>();
+  // two half-size intermediates when the rows need more than one tile of each
+  const size_t per = (size_t)B * Op::NARR << log2L;
+  bool dual = SSQB_DUAL_STREAM && zcap / 2 >= per && (size_t)nrows * per > zcap / 2;
+  const bool dry = launch_counter() != nullptr;
+  AuxStream* ax = (dual && !dry) ? aux_stream() : nullptr;
+  if (dual && !dry && !ax) dual = false;
+  const size_t cap = dual ? zcap / 2 : zcap;
+  const int S = rows_per_tile(cap, B, Op::NARR, log2L, nrows, cpr, 2 * sms);
+  if (!dual || dry) {
+    int t = 0;
+    for (int r0 = 0; r0 < nrows; r0 += S, ++t) {
+      const int e = run_rows<Op, C, SIGN>(op, B, log2L, Z + (dual ? (t & 1) * cap : 0), r0,
+                                          (nrows - r0) < S ? (nrows - r0) : S, tb, st);
+      if (e) return e;
+    }
+    return 0;
+  }
+  cudaError_t ce = cudaEventRecord(ax->fork, st);
+  if (!ce) ce = cudaStreamWaitEvent(ax->s, ax->fork, 0);
+  if (ce) return ce;
+  int e = 0;
+  int t = 0;
+  for (int r0 = 0; r0 < nrows && !e; r0 += S, ++t) {
+    const int rows = (nrows - r0) < S ? (nrows - r0) : S;
+    e = run_rows<Op, C, SIGN>(op, B, log2L, Z + (t & 1) * cap, r0, rows, tb,
+                              (t & 1) ? ax->s : st);
+  }
+  // join even after a failed launch, so the caller's stream never runs ahead
+  ce = cudaEventRecord(ax->join, ax->s);
+  if (!ce) ce = cudaStreamWaitEvent(st, ax->join, 0);
+  return e ? e : (int)ce;
 }
 
 // Batches: signals go through in chunks whose two-pass intermediate fits
@@ -121,8 +145,10 @@ static int run_batch(BOp op, int nsig, int nrows, int log2L, C* Z, size_t zcap,
                      const Tables& tb, cudaStream_t st) {
   int chunk = nsig;
   if (two_pass<C>(log2L)) {
+    // chunks of signals whose row fits half the intermediate, so that row
+    // tiles can alternate between two streams
     const size_t per = (size_t)BOp::NARR << log2L;
-    const size_t c = zcap / per;
+    const size_t c = (SSQB_DUAL_STREAM ? zcap / 2 : zcap) / per;
     chunk = c < 1 ? 1 : (c > (size_t)nsig ? nsig : (int)c);
   }
   const size_t Npad = (size_t)1 << log2L;
@@ -132,6 +158,34 @@ static int run_batch(BOp op, int nsig, int nrows, int log2L, C* Z, size_t zcap,
     o.xh += (size_t)s0 * Npad;
     const int n = (nsig - s0) < chunk ? (nsig - s0) : chunk;
     const int e = run_tile<BOp, C, SIGN>(o, n, nrows, log2L, Z, zcap, tb, st);
+    if (e) return e;
+  }
+  return 0;
+}
+
+// Signals of one call in chunks when all of them need more than half of the
+// intermediate per row: each chunk's row fits half of the L2 budget, so its
+// row tiles alternate between two streams (ops with `shifted(b0)`).
+#ifndef SSQB_CHUNK_SIGNALS
+#define SSQB_CHUNK_SIGNALS 1
+#endif
+template <class Op, typename C, int SIGN>
+static int run_tile_signals(const Op& op, int B, int nrows, int log2L, C* Z, size_t zcap,
+                            const Tables& tb, cudaStream_t st) {
+  const size_t per_sig = (size_t)Op::NARR << log2L;
+  if (!SSQB_CHUNK_SIGNALS || !SSQB_DUAL_STREAM || B < 2 || !two_pass<C>(log2L) ||
+      (size_t)B * per_sig <= zcap / 2)
+    return run_tile<Op, C, SIGN>(op, B, nrows, log2L, Z, zcap, tb, st);
+  const size_t half = (kZBudgetBytes / sizeof(C)) / 2;
+  size_t bc = half / per_sig;
+  if (bc < 1) bc = 1;
+  const int Bc = (int)bc;
+  size_t cap = 2 * bc * per_sig;
+  if (cap < kZBudgetBytes / sizeof(C)) cap = kZBudgetBytes / sizeof(C);
+  if (cap > zcap) cap = zcap;
+  for (int b0 = 0; b0 < B; b0 += Bc) {
+    const int n = (B - b0) < Bc ? (B - b0) : Bc;
+    const int e = run_tile<Op, C, SIGN>(op.shifted(b0), n, nrows, log2L, Z, cap, tb, st);
     if (e) return e;
   }
   return 0;
