@@ -490,9 +490,13 @@ int ssqb_cwt_noalloc(const void* x, int B, int N, int Npad, int n1, int padtype,
     }
     scratch = g_noalloc_ptr[dev];
   }
-  return ssqb_cwt(x, B, N, Npad, n1, padtype, rpadded, scales, na, wavelet, dt, bins, gamma,
-                  precision, Wx, dWx, w, idx, idx_pitch, scratch, kNoAllocScratchBytes,
-                  stream);
+  // one stream only: this entry point creates no stream or event either
+  set_aux_streams(false);
+  const int r = ssqb_cwt(x, B, N, Npad, n1, padtype, rpadded, scales, na, wavelet, dt, bins,
+                         gamma, precision, Wx, dWx, w, idx, idx_pitch, scratch,
+                         kNoAllocScratchBytes, stream);
+  set_aux_streams(true);
+  return r;
 }
 
 size_t ssqb_cwt_noalloc_max_bytes(void) { return kNoAllocScratchBytes; }

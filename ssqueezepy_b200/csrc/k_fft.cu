@@ -9,7 +9,11 @@ static thread_local int* t_count = nullptr;
 void set_launch_counter(int* c) { t_count = c; }
 int* launch_counter() { return t_count; }
 
+static thread_local bool t_aux_off = false;
+void set_aux_streams(bool on) { t_aux_off = !on; }
+
 AuxStream* aux_stream() {
+  if (t_aux_off) return nullptr;
   static thread_local AuxStream t_aux[256];
   static thread_local bool t_made[256], t_bad[256];
   int dev = 0;

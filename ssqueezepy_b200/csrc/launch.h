@@ -50,7 +50,8 @@ struct AuxStream {
   cudaStream_t s;
   cudaEvent_t fork, join;
 };
-AuxStream* aux_stream();  // NULL if it cannot be created
+AuxStream* aux_stream();  // NULL if it cannot be created or is switched off
+void set_aux_streams(bool on);  // this host thread; on by default
 
 // single pass when L fits one tile (4096 float2 / 2048 double2 elements);
 // else two passes with log2(L2) = m/2
