@@ -267,6 +267,24 @@ SSQB_API int ssqb_cwt_adjoint(const void* gWx, const void* gTx, const uint16_t* 
                               int accumulate, void* workspace, size_t workspace_bytes,
                               void* stream);
 
+/* Workspace bytes of ssqb_stft_adjoint: the real per-frame inverse
+ * transforms, B * n_fft * n_frames elements of the data precision. */
+SSQB_API size_t ssqb_stft_adjoint_workspace_bytes(int B, int N, int n_fft, int hop,
+                                                  int precision);
+
+/* Gradient of x through Sx = stft(x) (the transposed STFT of ssqb_stft's
+ * framing, window and one-sided FFT): per frame the real part of the
+ * inverse transform of the one-sided gradient, times the window, added back
+ * at the frame's samples, then the transpose of the padding. The gradient of
+ * Sx is gSx (B, n_fft/2+1, n_frames) and / or, through the squeeze, gTx with
+ * the forward's idx and sq_weights (as in ssqb_cwt_adjoint). window is the
+ * forward's (n_fft) window (double, device); geometry as in ssqb_stft. */
+SSQB_API int ssqb_stft_adjoint(const void* gSx, const void* gTx, const uint16_t* idx,
+                               int idx_pitch, const double* sq_weights, int B, int N,
+                               int n_fft, int hop, int n1, int padtype, int modulated,
+                               const double* window, int precision, void* gx, int accumulate,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* Gradient of Wx through the squeeze, a gather through the bin index:
  * gWx[b, i, j] = row_weights[i] * gTx[b, idx[b, i, j], j] (0 where idx is
  * 0xFFFF). Transpose of ssqb_squeeze. */

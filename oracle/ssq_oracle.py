@@ -378,3 +378,38 @@ def icwt_adjoint(gx, weights):
     x = sum_i weights[i] Re Wx[i] (+ mean): weights[i] * gx (real)."""
     w = np.asarray(weights, np.float64).reshape(-1, 1)
     return (w * np.asarray(gx, np.float64)[..., None, :]).astype(np.complex128)
+
+
+def stft_adjoint(gS, window, n_fft, N, hop=1, padtype='reflect', modulated=True):
+    """Gradient of x (..., N) for a gradient gS (..., n_fft//2+1, n_frames)
+    of Sx = stft(x)[0] (the transpose of `frames`, the window and `rfft`)."""
+    gS = np.asarray(gS, np.complex128)
+    L = n_fft
+    nfr = gS.shape[-1]
+    G = np.zeros(gS.shape[:-2] + (L, nfr), np.complex128)
+    G[..., :L // 2 + 1, :] = gS
+    gu = (sfft.ifft(G, axis=-2, workers=_WORKERS) * L).real   # (..., L, n_frames)
+    win = np.asarray(window, np.float64)
+    if modulated:
+        win = np.fft.ifftshift(win)
+    gF = gu * win.reshape(-1, 1)
+    padlength = N + n_fft - 1
+    if abs(padlength - N) % 2 == 0:
+        n1 = n2 = (padlength - N) // 2
+    else:
+        n2 = (padlength - N) // 2
+        n1 = n2 + 1
+    s20 = int(np.ceil(n_fft / 2))
+    s21 = s20 - 1 if n_fft % 2 == 1 else s20
+    m = np.arange(n_fft)
+    srcm = np.where(m < s20, m + s21, m - s20) if modulated else m
+    pos = hop * np.arange(nfr)[None, :] + srcm[:, None]            # padded position
+    src = pad_sources(N, padtype, n1, n2)
+    gF2 = gF.reshape(-1, L, nfr)
+    out = np.zeros((gF2.shape[0], N))
+    for b in range(gF2.shape[0]):
+        gxp = np.zeros(padlength)
+        np.add.at(gxp, pos.ravel(), gF2[b].ravel())
+        keep = src >= 0
+        np.add.at(out[b], src[keep], gxp[keep])
+    return out.reshape(gS.shape[:-2] + (N,))

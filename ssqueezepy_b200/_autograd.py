@@ -15,6 +15,10 @@ calls the adjoint kernels of libssqb.so:
   index of the forward, never Wx.
 * `icwt`: each row receives its weight times the output gradient
   (`ssqb_icwt_adjoint`).
+* `stft` / `ssq_stft`: the transposed STFT (`ssqb_stft_adjoint`): per frame
+  the real part of the inverse transform of the one-sided gradient, times
+  the window, added back at the frame's samples, then the transpose of the
+  padding; `ssq_stft`'s squeeze gather is fused into its loader.
 
 Gradients of float32 transforms are computed in float32 arithmetic.
 """
@@ -94,6 +98,72 @@ class SsqCwtFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gTx, gWx):
         gx = cwt_adjoint(ctx.r, gWx=gWx, gTx=gTx, sq_weights=ctx.cst)
+        shape, dtype = ctx.x_meta
+        return gx.reshape(shape).to(dtype), None
+
+
+def stft_adjoint(r, gSx=None, gTx=None, sq_weights=None):
+    """Gradient of x (B, N) from the gradients of Sx / Tx of the STFT forward
+    described by `r` (the dict of `_stft_core`)."""
+    B, N, nrow, nf = r['B'], r['N'], r['nrow'], r['nframes']
+    dev = r['dev']
+    rdt = torch.float64 if r['prec'] == L.F64 else torch.float32
+    cdt = torch.complex128 if r['prec'] == L.F64 else torch.complex64
+    gx = torch.empty((B, N), dtype=rdt, device=dev)
+    if gSx is None and gTx is None:
+        return gx.zero_()
+    lib = L.load()
+    wsb = lib.ssqb_stft_adjoint_workspace_bytes(B, N, r['n_fft'], r['hop'], r['prec'])
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    gSx = None if gSx is None else gSx.to(cdt).reshape(B, nrow, nf).contiguous()
+    gTx = None if gTx is None else gTx.to(cdt).reshape(B, nrow, nf).contiguous()
+    with torch.cuda.device(dev):
+        rc = lib.ssqb_stft_adjoint(
+            L.ptr(gSx), L.ptr(gTx), L.ptr(r['idx'] if gTx is not None else None),
+            r['ipitch'], L.ptr(sq_weights if gTx is not None else None), B, N, r['n_fft'],
+            r['hop'], r['n1'], r['ptype'], 1 if r['modulated'] else 0, L.ptr(r['wd']),
+            r['prec'], L.ptr(gx), 0, L.ptr(ws), wsb, L.stream_ptr())
+    L.check(rc, 'stft_adjoint')
+    return gx
+
+
+def _keep_stft(r):
+    return {k: v for k, v in r.items() if k not in ('Sx', 'dSx', 'w')}
+
+
+class StftFn(torch.autograd.Function):
+    """x -> Sx (and a non-differentiable dSx when the forward returns it)."""
+
+    @staticmethod
+    def forward(ctx, x, run):
+        r = run(x)
+        ctx.r = _keep_stft(r)
+        ctx.x_meta = (x.shape, x.dtype)
+        if r['dSx'] is not None:
+            ctx.mark_non_differentiable(r['dSx'])
+            return r['Sx'], r['dSx']
+        return r['Sx']
+
+    @staticmethod
+    def backward(ctx, gSx, *rest):
+        gx = stft_adjoint(ctx.r, gSx=gSx)
+        shape, dtype = ctx.x_meta
+        return gx.reshape(shape).to(dtype), None
+
+
+class SsqStftFn(torch.autograd.Function):
+    """x -> (Tx, Sx); the backward needs only the forward's bin index."""
+
+    @staticmethod
+    def forward(ctx, x, run):
+        Tx, r, cst = run(x)
+        ctx.r, ctx.cst = _keep_stft(r), cst
+        ctx.x_meta = (x.shape, x.dtype)
+        return Tx, r['Sx']
+
+    @staticmethod
+    def backward(ctx, gTx, gSx):
+        gx = stft_adjoint(ctx.r, gSx=gSx, gTx=gTx, sq_weights=ctx.cst)
         shape, dtype = ctx.x_meta
         return gx.reshape(shape).to(dtype), None
 

@@ -61,6 +61,9 @@ SIGNATURES = {
     'ssqb_cwt_adjoint': (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _vp, _i, _i, _i, _i, _i,
                               _vp, _i, ctypes.POINTER(CWavelet), _i, _vp, _i, _vp, _sz,
                               _vp]),
+    'ssqb_stft_adjoint_workspace_bytes': (_sz, [_i, _i, _i, _i, _i]),
+    'ssqb_stft_adjoint': (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _i,
+                               _vp, _i, _vp, _sz, _vp]),
     'ssqb_squeeze_adjoint': (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _i, _vp]),
     'ssqb_icwt_adjoint': (_i, [_vp, _vp, _i, _i, _i, _i, _vp, _i, _vp]),
     'ssqb_squeeze_batch': (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),

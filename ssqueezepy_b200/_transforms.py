@@ -637,17 +637,32 @@ def _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
                                 L.ptr(idx), ipitch, L.stream_ptr())
     L.check(rc, 'stft')
     return dict(Sx=Sx, dSx=dSx, w=w, idx=idx, ipitch=ipitch, Sfs=Sfs, dtype=dtype,
-                dev=dev,
-                is_2d=is_2d, B=B, nrow=nrow, nframes=nframes, fs=fs, gamma=gamma)
+                dev=dev, is_2d=is_2d, B=B, nrow=nrow, nframes=nframes, fs=fs, gamma=gamma,
+                N=N, n_fft=n_fft, hop=hop_len, n1=n1, ptype=L.PADTYPES[padtype],
+                modulated=modulated, wd=wd, prec=_prec(dtype))
 
 
 def stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=None,
          padtype='reflect', modulated=True, derivative=False, dtype=None):
     """Short-Time Fourier Transform; returns `Sx` or `(Sx, dSx)`, CUDA tensors
     of shape (n_fft//2 + 1, n_frames) (_stft.py:13-181)."""
-    r = _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
-                   derivative, dtype)
-    Sx, dSx = _out(r['Sx'], True, r['is_2d']), _out(r['dSx'], True, r['is_2d'])
+    def run(xin):
+        return _stft_core(xin, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
+                          derivative, dtype)
+    if A.needs_grad(x):
+        _grad_checks(True, False, padtype)
+        holder = {}
+
+        def run_keep(xin):
+            holder['r'] = run(xin)
+            return holder['r']
+        outs = A.StftFn.apply(x, run_keep)
+        r = holder['r']
+        S, dS = outs if derivative else (outs, None)
+    else:
+        r = run(x)
+        S, dS = r['Sx'], r['dSx']
+    Sx, dSx = _out(S, True, r['is_2d']), _out(dS, True, r['is_2d'])
     return (Sx, dSx) if derivative else Sx
 
 
@@ -669,17 +684,34 @@ def ssq_stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=Non
     Sfs_np = np.linspace(0, .5 * fs_, nrow)
     f = Sfs_np if ssq_freqs is None else P._to_numpy(ssq_freqs).astype(np.float64).ravel()
     mode, bp = P.bin_params(f, False)
-    r = _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
-                   get_dWx, dtype, want_idx=True, want_w=get_w, bins=(mode, bp),
-                   gamma=gamma, flipud=flipud)
     const = P.squeeze_weights(None, None, None, 'stft', ssq_freqs=f)
-    Tx = torch.empty_like(r['Sx'])
-    cst = _dev_f64(const, r['dev'])
-    with torch.cuda.device(r['dev']):
-        rc = L.load().ssqb_squeeze(L.ptr(r['Sx']), L.ptr(r['idx']), r['ipitch'],
-                                   L.ptr(cst), r['B'], r['nrow'], r['nframes'], r['nrow'],
-                                   _prec(r['dtype']), L.ptr(Tx), L.stream_ptr())
-    L.check(rc, 'squeeze')
+
+    def run(xin):
+        r = _stft_core(xin, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
+                       get_dWx, dtype, want_idx=True, want_w=get_w, bins=(mode, bp),
+                       gamma=gamma, flipud=flipud)
+        Tx = torch.empty_like(r['Sx'])
+        cst = _dev_f64(const, r['dev'])
+        with torch.cuda.device(r['dev']):
+            rc = L.load().ssqb_squeeze(L.ptr(r['Sx']), L.ptr(r['idx']), r['ipitch'],
+                                       L.ptr(cst), r['B'], r['nrow'], r['nframes'],
+                                       r['nrow'], _prec(r['dtype']), L.ptr(Tx),
+                                       L.stream_ptr())
+        L.check(rc, 'squeeze')
+        return Tx, r, cst
+
+    if A.needs_grad(x):
+        _grad_checks(astensor, False, padtype)
+        holder = {}
+
+        def run_keep(xin):
+            holder['out'] = run(xin)
+            return holder['out']
+        Tx, Sx = A.SsqStftFn.apply(x, run_keep)
+        r = holder['out'][1]
+    else:
+        Tx, r, _ = run(x)
+        Sx = r['Sx']
     is2 = r['is_2d']
     Sfs_out = Sfs_np.astype(r['dtype'])
     f_out = f.astype(r['dtype']) if ssq_freqs is None else f
@@ -688,7 +720,7 @@ def ssq_stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=Non
     if astensor:
         Sfs_out = torch.as_tensor(Sfs_out, device=r['dev'])
         f_out = torch.as_tensor(np.ascontiguousarray(f_out), device=r['dev'])
-    out = [_out(Tx, astensor, is2), _out(r['Sx'], astensor, is2), f_out, Sfs_out]
+    out = [_out(Tx, astensor, is2), _out(Sx, astensor, is2), f_out, Sfs_out]
     if get_w:
         out.append(_out(r['w'], astensor, is2))
     if get_dWx:

@@ -225,9 +225,16 @@ size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
   if (cwt_two_pass(ilog2i(Npad), precision)) {
     const size_t per_row = (size_t)B * 2 * Npad * csize(precision);
     size_t rows = kZBudgetBytes / per_row;
-    if (rows < 1) rows = 1;
+    if (rows < 2) rows = 2;  // two row tiles, one per stream
     if (rows > (size_t)na) rows = na;
     z = rows * per_row;
+    if (B > 1 && per_row > kZBudgetBytes / 2) {
+      // signals go in chunks whose two row tiles fit the budget
+      const size_t per_sig = 2 * (size_t)Npad * csize(precision);
+      size_t bc = kZBudgetBytes / 2 / per_sig;
+      if (bc < 1) bc = 1;
+      z = 2 * bc * per_sig > kZBudgetBytes ? 2 * bc * per_sig : kZBudgetBytes;
+    }
     const size_t mz = min_z_bytes(B, Npad, precision);
     if (z < mz) z = mz;
   }
@@ -668,6 +675,62 @@ int ssqb_cwt_adjoint(const void* gWx, const void* gTx, const uint16_t* idx, int 
                             accumulate, workspace, workspace_bytes, tb, st);
   }
   if (e) return cuda_fail((cudaError_t)e, "cwt adjoint launch");
+  return SSQB_OK;
+}
+
+size_t ssqb_stft_adjoint_workspace_bytes(int B, int N, int n_fft, int hop, int precision) {
+  if (B < 1 || N < 1 || hop < 1 || !is_pow2(n_fft) || !valid_precision(precision)) return 0;
+  const size_t rs = data_prec(precision) == SSQB_F64 ? sizeof(double) : sizeof(float);
+  return (size_t)B * n_fft * ((size_t)(N - 1) / hop + 1) * rs;
+}
+
+int ssqb_stft_adjoint(const void* gSx, const void* gTx, const uint16_t* idx, int idx_pitch,
+                      const double* sq_weights, int B, int N, int n_fft, int hop, int n1,
+                      int padtype, int modulated, const double* window, int precision,
+                      void* gx, int accumulate, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+  if (!window || !gx || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || hop < 1) return fail(SSQB_EINVAL, "B, N and hop must be >= 1");
+  if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  if (!is_pow2(n_fft) || n_fft < 8 || n_fft > 4096)
+    return fail(SSQB_EUNSUPPORTED, "n_fft must be a power of two in [8, 4096]");
+  const bool f64 = data_prec(precision) == SSQB_F64;
+  if (f64 && n_fft > FftCfg<double2>::TILE)
+    return fail(SSQB_EUNSUPPORTED, "n_fft above " + std::to_string(FftCfg<double2>::TILE) +
+                                       " needs float32 data");
+  if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
+  if (padtype == 3)
+    return fail(SSQB_EUNSUPPORTED, "the adjoint of replicate padding is not implemented");
+  if (n1 < 0 || n1 > n_fft) return fail(SSQB_EINVAL, "bad padding geometry");
+  const int nframes = (N - 1) / hop + 1;
+  if (idx_pitch == 0) idx_pitch = nframes;
+  const int nrow = n_fft / 2 + 1;
+  int r = check_adj_sources(gSx, gTx, idx, idx_pitch, sq_weights, nrow, nullptr, nullptr,
+                            nframes);
+  if (r) return r;
+  const size_t need = ssqb_stft_adjoint_workspace_bytes(B, N, n_fft, hop, precision);
+  if (workspace_bytes < need)
+    return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                     " bytes");
+  Tables tb;
+  r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  int e;
+  if (f64) {
+    AdjSources<double2> src{(const double2*)gSx, (const double2*)gTx, idx, idx_pitch, nrow,
+                            sq_weights, nullptr, nullptr};
+    e = run_stft_adjoint_f64(src, B, N, n_fft, hop, n1, padtype, modulated ? 1 : 0, window,
+                             (double*)gx, accumulate, workspace, tb, st);
+  } else {
+    AdjSources<float2> src{(const float2*)gSx, (const float2*)gTx, idx, idx_pitch, nrow,
+                           sq_weights, nullptr, nullptr};
+    e = run_stft_adjoint_f32(src, B, N, n_fft, hop, n1, padtype, modulated ? 1 : 0, window,
+                             (float*)gx, accumulate, workspace, tb, st);
+  }
+  if (e) return cuda_fail((cudaError_t)e, "stft adjoint launch");
   return SSQB_OK;
 }
 

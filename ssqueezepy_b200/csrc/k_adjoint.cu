@@ -82,9 +82,34 @@ struct AdjInvOp {
   }
 };
 
+// Calls f(q) for every padded offset q in [qlo, qhi) (relative to x[0])
+// whose source sample is s: q = s first, then the images of the padding's
+// one or two residue families (period P), ascending.
+template <class F>
+__device__ __forceinline__ void for_each_image(int s, int N, long long qlo, long long qhi,
+                                               int padtype, const F& f) {
+  if (s >= qlo && s < qhi) f((long long)s);
+  long long P = 1, a[2] = {s, s};
+  int nf = 0;
+  if (padtype == PAD_REFLECT && N > 1) { P = 2LL * (N - 1); a[0] = s; a[1] = -s; nf = 2; }
+  else if (padtype == PAD_SYMMETRIC) { P = 2LL * N; a[0] = s; a[1] = -1 - s; nf = 2; }
+  else if (padtype == PAD_WRAP) { P = N; a[0] = s; nf = 1; }
+  for (int fam = 0; fam < nf; ++fam) {
+    // k from ceil((qlo - a) / P) to floor((qhi - 1 - a) / P)
+    const long long lo = qlo - a[fam], hi = qhi - 1 - a[fam];
+    const long long k0 = lo >= 0 ? (lo + P - 1) / P : -((-lo) / P);
+    for (long long k = k0; k * P <= hi; ++k) {
+      const long long q = a[fam] + k * P;
+      if (q >= 0 && q < N) continue;                            // the signal itself
+      if (fam == 1 && ((q - a[0]) % P + P) % P == 0) continue;  // already in family 0
+      if (pad_src(q, N, padtype) != s) continue;
+      f(q);
+    }
+  }
+}
+
 // gx[b, s] (+)= sum of yp[b, n1 + q] over the padded offsets q whose source
-// is s (pad_src(q) == s): q = s, then the images q = a + k P of the one or
-// two residue families of the padding, ascending k.
+// is s (the transpose of the padding).
 template <typename T>
 __global__ void adj_fold_kernel(const T* __restrict__ yp, int B, int N, int Npad, int n1,
                                 int padtype, T* __restrict__ gx, int accumulate) {
@@ -92,25 +117,62 @@ __global__ void adj_fold_kernel(const T* __restrict__ yp, int B, int N, int Npad
   if (i >= (size_t)B * N) return;
   const int b = (int)(i / N), s = (int)(i % N);
   const T* y = yp + (size_t)b * Npad + n1;
-  T acc = y[s];
-  long long P = 1, a[2] = {s, s};
-  int nf = 0;
-  if (padtype == PAD_REFLECT && N > 1) { P = 2LL * (N - 1); a[0] = s; a[1] = -s; nf = 2; }
-  else if (padtype == PAD_SYMMETRIC) { P = 2LL * N; a[0] = s; a[1] = -1 - s; nf = 2; }
-  else if (padtype == PAD_WRAP) { P = N; a[0] = s; nf = 1; }
-  const long long qlo = -(long long)n1, qhi = (long long)Npad - n1;  // q in [qlo, qhi)
-  for (int f = 0; f < nf; ++f) {
-    // k from ceil((qlo - a) / P) to floor((qhi - 1 - a) / P)
-    const long long lo = qlo - a[f], hi = qhi - 1 - a[f];
-    const long long k0 = lo >= 0 ? (lo + P - 1) / P : -((-lo) / P);
-    for (long long k = k0; k * P <= hi; ++k) {
-      const long long q = a[f] + k * P;
-      if (q >= 0 && q < N) continue;                          // the signal itself
-      if (f == 1 && ((q - a[0]) % P + P) % P == 0) continue;  // already in family 0
-      if (pad_src(q, N, padtype) != s) continue;
-      acc += y[q];
-    }
+  T acc = 0;
+  for_each_image(s, N, -(long long)n1, (long long)Npad - n1, padtype,
+                 [&](long long q) { acc += y[q]; });
+  gx[i] = accumulate ? gx[i] + acc : acc;
+}
+
+// ---- STFT adjoint ------------------------------------------------------------
+// Forward: frame t, element m, u[t, m] = xp[t hop + q(m)] win[q(m)] with
+// q(m) = (m + s21) mod L (modulated) or m; Sx[f, t] = sum_m u[t, m] e^{-2 pi i f m / L}
+// for f <= L/2. Adjoint: gu[t, m] = Re sum_{f <= L/2} g[f, t] e^{+2 pi i f m / L},
+// then gx[s] = sum over the frames and elements reading s of win[q] gu[t, m].
+template <typename C>
+struct StftAdjOp {
+  typedef typename RealOf<C>::type T;
+  static constexpr int NARR = 1;
+  static constexpr bool kDirect = false;
+  static constexpr bool kBatch = false;
+  static constexpr int kMapIn = MAP_F;  // consecutive threads: consecutive frames
+  AdjSources<C> src;                    // gradient of Sx (B, nrow, nframes)
+  int L, nrow, nframes;
+  T* gu;                                // (B, L, nframes), element-major
+  int* status;
+  __device__ StftAdjOp bind(int) const { return *this; }
+  __device__ int rows() const { return nframes; }
+  __device__ void load(int b, int t, int f, C (&v)[1]) const {
+    v[0] = f < nrow ? src.at(b, nrow, nframes, f, t, status) : mk((T)0, (T)0);
   }
+  template <class LY>
+  __device__ void store_smem(int b, int t, int n, C* const (&buf)[1], int fr) const {
+    gu[((size_t)b * L + n) * nframes + t] = buf[0][LY::at(fr, n)].x;
+  }
+};
+
+template <typename T>
+__global__ void stft_adj_gather_kernel(const T* __restrict__ gu, const double* __restrict__ win,
+                                       int B, int N, int L, int hop, int nframes, int n1,
+                                       int padtype, int modulated, int s21,
+                                       T* __restrict__ gx, int accumulate) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)B * N) return;
+  const int b = (int)(i / N), s = (int)(i % N);
+  const T* g = gu + (size_t)b * L * nframes;
+  const long long ptot = (long long)(nframes - 1) * hop + L;  // padded positions read
+  T acc = 0;
+  for_each_image(s, N, -(long long)n1, ptot - n1, padtype, [&](long long qq) {
+    const long long p = qq + n1;
+    const long long num = p - L + 1;
+    const long long tlo = num <= 0 ? 0 : (num + hop - 1) / hop;
+    long long thi = p / hop;
+    if (thi > nframes - 1) thi = nframes - 1;
+    for (long long t = thi; t >= tlo; --t) {
+      const int q = (int)(p - t * hop);
+      const int m = modulated ? ((q - s21) & (L - 1)) : q;
+      acc += (T)__ldg(win + q) * g[(size_t)m * nframes + t];
+    }
+  });
   gx[i] = accumulate ? gx[i] + acc : acc;
 }
 
@@ -188,6 +250,39 @@ static int run_adjoint(const AdjSources<C>& src, int B, int N, int Npad, int n1,
   adj_fold_kernel<T><<<(unsigned)((n + nt - 1) / nt), nt, 0, st>>>(yp, B, N, Npad, n1, padtype,
                                                                     gx, accumulate);
   return cudaGetLastError();
+}
+
+template <typename C>
+static int run_stft_adj(const AdjSources<C>& src, int B, int N, int L, int hop, int n1,
+                        int padtype, int modulated, const double* win,
+                        typename RealOf<C>::type* gx, int accumulate, void* ws,
+                        const Tables& tb, cudaStream_t st) {
+  typedef typename RealOf<C>::type T;
+  const int nframes = (N - 1) / hop + 1;
+  StftAdjOp<C> op{src, L, L / 2 + 1, nframes, (T*)ws, tb.status};
+  int e = run_single<StftAdjOp<C>, C, 1>(op, B, nframes, ilog2(L), tb, st);
+  if (e) return e;
+  if (int* c = launch_counter()) return ++*c, 0;
+  const int s20 = (L + 1) / 2;
+  const int s21 = (L % 2 == 1) ? s20 - 1 : s20;
+  const size_t n = (size_t)B * N;
+  stft_adj_gather_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+      (const T*)ws, win, B, N, L, hop, nframes, n1, padtype, modulated, s21, gx, accumulate);
+  return cudaGetLastError();
+}
+
+int run_stft_adjoint_f32(const AdjSources<float2>& src, int B, int N, int L, int hop, int n1,
+                         int padtype, int modulated, const double* win, float* gx,
+                         int accumulate, void* ws, const Tables& tb, cudaStream_t st) {
+  return run_stft_adj<float2>(src, B, N, L, hop, n1, padtype, modulated, win, gx, accumulate,
+                              ws, tb, st);
+}
+
+int run_stft_adjoint_f64(const AdjSources<double2>& src, int B, int N, int L, int hop, int n1,
+                         int padtype, int modulated, const double* win, double* gx,
+                         int accumulate, void* ws, const Tables& tb, cudaStream_t st) {
+  return run_stft_adj<double2>(src, B, N, L, hop, n1, padtype, modulated, win, gx, accumulate,
+                               ws, tb, st);
 }
 
 int run_cwt_adjoint_f32(const AdjSources<float2>& src, int B, int N, int Npad, int n1,

@@ -120,6 +120,12 @@ int run_cwt_adjoint_f64(const AdjSources<double2>& src, int B, int N, int Npad, 
                         int padtype, const double* scales, int na, const WavDev& wd,
                         double* gx, int accumulate, void* ws, size_t ws_bytes,
                         const Tables& tb, cudaStream_t st);
+int run_stft_adjoint_f32(const AdjSources<float2>& src, int B, int N, int L, int hop, int n1,
+                         int padtype, int modulated, const double* win, float* gx,
+                         int accumulate, void* ws, const Tables& tb, cudaStream_t st);
+int run_stft_adjoint_f64(const AdjSources<double2>& src, int B, int N, int L, int hop, int n1,
+                         int padtype, int modulated, const double* win, double* gx,
+                         int accumulate, void* ws, const Tables& tb, cudaStream_t st);
 int run_wx_adjoint_f32(const AdjSources<float2>& src, int B, int na, int N, float2* gWx,
                        int accumulate, int* status, cudaStream_t st);
 int run_wx_adjoint_f64(const AdjSources<double2>& src, int B, int na, int N, double2* gWx,

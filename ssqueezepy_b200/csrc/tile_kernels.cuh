@@ -84,6 +84,12 @@ struct Pass1Store {
   }
 };
 
+// Mapping of the first stage of tile_single: MAP_J unless the op asks for
+// rows-fastest loads (kMapIn = MAP_F, e.g. inputs stored frame-minor).
+template <class T, class = void> struct MapIn { static constexpr int value = MAP_J; };
+template <class T>
+struct MapIn<T, std::void_t<decltype(T::kMapIn)>> { static constexpr int value = T::kMapIn; };
+
 // Pass-1 loader: input k1_0 + f + L1*m of row `row`. Ops with a split load
 // get a gather that issues the R spectrum loads of an item (only those in
 // the row's wavelet band) before any wavelet arithmetic.
@@ -154,12 +160,13 @@ tile_single(Op op, Tables tb) {
     }
   };
   typedef decltype(op.bind(0)) BOp;
+  constexpr int MI = MapIn<BOp>::value;
   if constexpr (Op::kDirect) {
     StoreEach<BOp, C> st{bop, b, row0, nrows, 1, 0};
-    fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, true>(buf, seg_table<C>(tb), ld, st);
+    fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MI, MAP_J, true>(buf, seg_table<C>(tb), ld, st);
   } else {
     StoreEach<BOp, C> st{bop, b, row0, nrows, 1, 0};
-    fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MAP_J, MAP_J, false>(buf, seg_table<C>(tb), ld, st);
+    fft_rows<C, LOGL, NF, kNT, SIGN, NARR, MI, MAP_J, false>(buf, seg_table<C>(tb), ld, st);
     for (int e = threadIdx.x; e < TILE; e += kNT) {
       const int f = e % NF, n = e / NF;  // rows fastest: coalesced (row, n) outputs
       if (row0 + f < nrows) bop.template store_smem<LY>(b, row0 + f, n, buf, f);

@@ -1,6 +1,7 @@
 # -*- coding: utf-8 -*-
-"""Reverse-mode differentiation: the adjoint kernels behind `cwt`, `ssq_cwt`
-and `icwt` (ssqb_cwt_adjoint, ssqb_squeeze_adjoint, ssqb_icwt_adjoint).
+"""Reverse-mode differentiation: the adjoint kernels behind `cwt`, `ssq_cwt`,
+`icwt`, `stft` and `ssq_stft` (ssqb_cwt_adjoint, ssqb_stft_adjoint,
+ssqb_squeeze_adjoint, ssqb_icwt_adjoint).
 
 CPU: argument checks of the adjoint entry points (no device call).
 GPU: each adjoint against the float64 oracle's transposes (which the CPU
@@ -237,3 +238,56 @@ def test_training_loss_gradient_vs_finite_differences_and_torch_composite():
     e_tc = np.linalg.norm(g_ours - g_ref) / np.linalg.norm(g_ref)
     assert e_tc <= 1e-4, e_tc
     assert abs(float(loss) - float(lt)) <= 1e-4 * abs(float(lt))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+@pytest.mark.parametrize('hop, padtype', [(1, 'reflect'), (2, 'zero'), (3, 'reflect')])
+def test_stft_backward_matches_oracle_adjoint(dtype, hop, padtype):
+    torch = _torch()
+    import ssqueezepy_b200 as sb
+    from oracle import ssq_oracle as O
+    from scipy.signal import get_window
+    N, n_fft = 3000, 256
+    rng = np.random.default_rng(hop)
+    x = torch.tensor(S.same_length_batch(2, N, 3), device='cuda',
+                     dtype=getattr(torch, dtype), requires_grad=True)
+    Sx = sb.stft(x, window='hann', n_fft=n_fft, hop_len=hop, padtype=padtype, dtype=dtype)
+    g = rng.standard_normal(Sx.shape) + 1j * rng.standard_normal(Sx.shape)
+    (gx,) = torch.autograd.grad(Sx, x, torch.as_tensor(g, dtype=Sx.dtype, device='cuda'))
+    win = get_window('hann', n_fft, fftbins=True)
+    ref = O.stft_adjoint(g, win, n_fft, N, hop=hop, padtype=padtype)
+    err = np.linalg.norm(gx.double().cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err <= (1e-5 if dtype == 'float32' else 1e-11), err
+    assert L.device_status() == 0
+
+
+@pytest.mark.gpu
+def test_ssq_stft_backward_is_gather_then_transpose():
+    torch = _torch()
+    import ssqueezepy_b200 as sb
+    from oracle import ssq_oracle as O
+    from scipy.signal import get_window
+    from ssqueezepy_b200 import _transforms as T
+    N, n_fft = 4000, 128
+    x = torch.tensor(S.same_length_batch(1, N, 4)[0], device='cuda', dtype=torch.float32,
+                     requires_grad=True)
+    Tx, Sx, f, Sfs = sb.ssq_stft(x, window='hann', n_fft=n_fft)
+    rng = np.random.default_rng(2)
+    gT = rng.standard_normal(Tx.shape) + 1j * rng.standard_normal(Tx.shape)
+    gS = rng.standard_normal(Sx.shape) + 1j * rng.standard_normal(Sx.shape)
+    (gx,) = torch.autograd.grad((Tx, Sx), x,
+                                (torch.as_tensor(gT, dtype=Tx.dtype, device='cuda'),
+                                 torch.as_tensor(gS, dtype=Sx.dtype, device='cuda')))
+    nrow = n_fft // 2 + 1
+    Sfs64 = np.linspace(0, .5, nrow)
+    mode, bp = P.bin_params(Sfs64, False)
+    r = T._stft_core(x.detach(), 'hann', n_fft, None, 1, None, None, 'reflect', True, False,
+                     'float32', want_idx=True, bins=(mode, bp))
+    k = r['idx'][0, :, :N].cpu().numpy().astype(np.int64)
+    use = k != L.NO_BIN
+    k = np.where(use, k, 0)
+    gStot = gS + O.squeeze_adjoint(gT, k, use, Sfs64[1] - Sfs64[0])
+    ref = O.stft_adjoint(gStot, get_window('hann', n_fft, fftbins=True), n_fft, N)
+    err = np.linalg.norm(gx.double().cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err <= 1e-5, err

@@ -131,3 +131,18 @@ def test_squeeze_and_icwt_adjoints_are_transposes():
     xr = (w[:, None] * W.real).sum(0)
     gW2 = O.icwt_adjoint(gx, w)
     assert abs(float(gx @ xr) - np.real(np.vdot(gW2, W))) < 1e-10 * np.abs(xr).sum()
+
+
+@pytest.mark.parametrize('padtype', ['reflect', 'zero'])
+@pytest.mark.parametrize('hop', [1, 3])
+def test_stft_adjoint_is_the_transpose(padtype, hop):
+    from scipy.signal import get_window
+    rng = np.random.default_rng(hop)
+    N, n_fft = 500, 64
+    win = get_window('hann', n_fft, fftbins=True)
+    x = rng.standard_normal(N)
+    Sx, _ = O.stft(x, win, win, n_fft, hop=hop, padtype=padtype)
+    g = rng.standard_normal(Sx.shape) + 1j * rng.standard_normal(Sx.shape)
+    gx = O.stft_adjoint(g, win, n_fft, N, hop=hop, padtype=padtype)
+    lhs = np.real(np.vdot(g, Sx))
+    assert abs(lhs - float(x @ gx)) <= 1e-10 * np.abs(g).sum() * np.abs(Sx).max()
