@@ -293,9 +293,9 @@ def run_e2e(sb, torch, dist, x_np, na, N, st, world, dev, barrier, args):
 
 def run_batched(args, torch, dev, world, barrier, flush):
     """256 float32 signals of lengths uniform in [4096, 65536] (seeded chirp
-    mixtures), Morlet mu=6, nv=32 log-piecewise: one SsqCwtBatch plan (a
-    CUDA graph per step) against one public ssq_cwt call per signal, both with
-    inputs resident on the device."""
+    mixtures), Morlet mu=6, nv=32 log-piecewise: one autotuned SsqCwtBatch
+    plan (a CUDA graph per step) against one public ssq_cwt call per signal,
+    both with inputs resident on the device."""
     import torch.distributed as dist
     import ssqueezepy_b200 as sb
     from ssqueezepy_b200._batch import SsqCwtBatch
@@ -305,7 +305,7 @@ def run_batched(args, torch, dev, world, barrier, flush):
           S.uneven_batch(args.batch, 4096, 65536, seed=1234 + rank)]
     lengths = [len(x) for x in xs]
     wav = ('morlet', {'mu': 6., 'dtype': 'float32'})
-    plan = SsqCwtBatch(lengths, wavelet=wav, graph=True, device=dev)
+    plan = SsqCwtBatch(lengths, wavelet=wav, graph=True, device=dev, autotune=True)
     plan.load(xs)
     st = torch.cuda.current_stream()
     for _ in range(max(args.warmup, 3)):
@@ -372,6 +372,7 @@ def run_batched(args, torch, dev, world, barrier, flush):
         "l2": "252 MB buffer written between timed steps; outputs %.1f GB"
               % (plan.n_out * 16 / 1e9),
         "Tx_rel_l2_vs_oracle_shortest_longest": tx_err,
+        "autotune": plan.tuning,
     }
 
 

@@ -77,11 +77,16 @@ class SsqCwtBatch:
     (packed input, Wx, Tx, bin index, workspace) belong to the plan, so each
     call overwrites the previous call's outputs. `graph=True` captures the
     device work in a CUDA graph after one eager run and replays it.
+    `autotune=True` picks, per padded-length group, the intermediate budget
+    (rows per tile and signals per chunk) that runs fastest on this device.
     """
+
+    # intermediate budgets the autotuner tries per length group, bytes
+    TUNE_BUDGETS = (32 << 20, 64 << 20, 128 << 20, 256 << 20)
 
     def __init__(self, lengths, wavelet='gmw', scales='log-piecewise', nv=32, fs=None,
                  padtype='reflect', maprange='peak', flipud=True, gamma=None,
-                 device=None, graph=False):
+                 device=None, graph=False, autotune=False):
         L.require_cuda()
         T._check_ssq_args('sum', maprange, 'trig')
         if padtype not in L.PADTYPES:
@@ -128,6 +133,11 @@ class SsqCwtBatch:
             ws = max(ws, lib.ssqb_cwt_batch_workspace_bytes(len(sel), int(Npad),
                                                             self.prec))
         self.sig_dev = self._to_dev(sig)
+        for g in self.groups:  # the library's default budget per group
+            g['ws'] = lib.ssqb_cwt_batch_workspace_bytes(g['n'], g['Npad'], self.prec)
+        if autotune:
+            xb = max(g['n'] * g['Npad'] * 16 for g in self.groups)
+            ws = max(ws, xb + max(self.TUNE_BUDGETS))
         self.ws_bytes = ws
         self.ws = torch.empty(ws, dtype=torch.uint8, device=dev)
         kind, *wp = wavelet.kernel_params()
@@ -140,6 +150,9 @@ class SsqCwtBatch:
         self.use_graph = graph
         self._graph = None
         self._ran = False
+        self.tuning = None
+        if autotune:
+            self.autotune()
 
     def _to_dev(self, arr):
         return torch.as_tensor(arr.view(np.uint8).copy(), device=self.dev)
@@ -151,11 +164,57 @@ class SsqCwtBatch:
         n = 1
         for g in self.groups:
             k = lib.ssqb_cwt_batch_launches(g['host'].ctypes.data_as(ctypes.c_void_p),
-                                            g['n'], g['Npad'], self.prec, self.ws_bytes)
+                                            g['n'], g['Npad'], self.prec, g['ws'])
             if k < 0:
                 raise RuntimeError("launch count query failed")
             n += k
         return n
+
+    def _cwt_group(self, g, ws_bytes, st):
+        lib = L.load()
+        rc = lib.ssqb_cwt_batch(
+            L.ptr(self.x), g['host'].ctypes.data_as(ctypes.c_void_p), L.ptr(g['dev']),
+            g['n'], g['Npad'], self.ptype, self.cw, float(self.dt), self.gamma, self.prec,
+            L.ptr(self.Wx), L.ptr(self.idx), L.ptr(self.ws), ws_bytes, st)
+        L.check(rc, 'cwt_batch')
+
+    def autotune(self, reps=2):
+        """Per length group, time the CWT under each intermediate budget of
+        TUNE_BUDGETS (which sets rows per tile and signals per chunk) with CUDA
+        events on the current stream, and keep the fastest. Runs on whatever
+        is in the packed input (the values do not change the work)."""
+        st = torch.cuda.current_stream(self.dev)
+        sp = L.stream_ptr(st)
+        if not self._ran:  # a seeded stand-in signal until the first load
+            gen = torch.Generator(device=self.dev)
+            gen.manual_seed(0)
+            self.x.copy_(torch.randn(self.n_x, generator=gen, device=self.dev))
+        self.tuning = []
+        for g in self.groups:
+            xb = g['n'] * g['Npad'] * 16
+            times = {}
+            for zb in self.TUNE_BUDGETS:
+                wsb = min(self.ws_bytes, xb + zb)
+                try:
+                    self._cwt_group(g, wsb, sp)  # warm (and too-small budgets refused)
+                except RuntimeError:
+                    continue
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                for _ in range(reps):
+                    self._cwt_group(g, wsb, sp)
+                e1.record(st)
+                e1.synchronize()
+                times[wsb] = e0.elapsed_time(e1) / reps
+            best = min(times, key=times.get)
+            g['ws'] = best
+            self.tuning.append(dict(Npad=g['Npad'], signals=g['n'],
+                                    budget_mb=(best - xb) / 2**20,
+                                    ms={round((k - xb) / 2**20): round(v, 3)
+                                        for k, v in times.items()}))
+        self._graph = None
+        return self.tuning
 
     def run(self):
         """The device work on the packed input `self.x` (graph replay once
@@ -178,12 +237,7 @@ class SsqCwtBatch:
         lib = L.load()
         st = L.stream_ptr()
         for g in self.groups:
-            rc = lib.ssqb_cwt_batch(
-                L.ptr(self.x), g['host'].ctypes.data_as(ctypes.c_void_p), L.ptr(g['dev']),
-                g['n'], g['Npad'], self.ptype, self.cw, float(self.dt), self.gamma,
-                self.prec, L.ptr(self.Wx), L.ptr(self.idx), L.ptr(self.ws),
-                self.ws_bytes, st)
-            L.check(rc, 'cwt_batch')
+            self._cwt_group(g, g['ws'], st)
         rc = lib.ssqb_squeeze_batch(
             L.ptr(self.Wx), L.ptr(self.idx), self.sig_np.ctypes.data_as(ctypes.c_void_p),
             L.ptr(self.sig_dev), len(self.lengths), self.prec, L.ptr(self.Tx), st)

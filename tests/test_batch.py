@@ -200,3 +200,21 @@ def test_batch_graph_replay_repeats_eager():
             assert torch.equal(t, t0) and torch.equal(w, w0)
     assert plan._graph is not None
     assert plan.launches >= 1 + 2 * 3
+
+
+@pytest.mark.gpu
+def test_batch_autotune_picks_a_budget_and_keeps_results():
+    torch = _gpu()
+    from ssqueezepy_b200._batch import SsqCwtBatch
+    rng = np.random.default_rng(9)
+    xs = [S.chirp_mix(N, rng).astype(np.float32) for N in LENGTHS]
+    ref = [(t.clone(), w.clone()) for t, w, _, _ in
+           SsqCwtBatch(LENGTHS, wavelet=('morlet', {'mu': 6.}))(xs)]
+    plan = SsqCwtBatch(LENGTHS, wavelet=('morlet', {'mu': 6.}), autotune=True, graph=True)
+    assert plan.tuning and all(t['ms'] for t in plan.tuning)
+    for _ in range(2):
+        outs = plan(xs)
+        torch.cuda.synchronize()
+        for (t, w, _, _), (t0, w0) in zip(outs, ref):
+            assert torch.equal(t, t0) and torch.equal(w, w0)
+    assert L.device_status() == 0
