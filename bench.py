@@ -108,6 +108,17 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def max_over_ranks(values, device):
+    """Element-wise max of per-rank timings over all ranks (every rank takes
+    the same collective; one rank returns its own values)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def oracle_step(x, scales, f_asc, const):
     from oracle import ssq_oracle as O
     return O.ssq_cwt(x, 'gmw_l1', (3., 60.), scales, f_asc, const)
@@ -232,10 +243,7 @@ def run_ours(args):
     cwt_ms = [e[0].elapsed_time(e[1]) for e in evs]
     sq_ms = [e[1].elapsed_time(e[2]) for e in evs]
     step_ms = float(np.sum(cwt_ms) + np.sum(sq_ms)) / args.steps
-    t_local = torch.tensor([step_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
-    step_ms_max = float(t_local.item())
+    step_ms_max, = max_over_ranks([step_ms], dev)
     value = world * N / (step_ms_max * 1e-3)
 
     # end to end through the public API from pinned host memory
@@ -284,11 +292,8 @@ def run_e2e(sb, torch, dist, x_np, na, N, st, world, dev, barrier, args):
         Tx_pin.copy_(Tp, non_blocking=True)
     e1.record(st)
     barrier()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1) / e2e_steps], dtype=torch.float64,
-                          device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    return world * N / (float(e2e_ms.item()) * 1e-3)
+    e2e_ms, = max_over_ranks([e0.elapsed_time(e1) / e2e_steps], dev)
+    return world * N / (e2e_ms * 1e-3)
 
 
 def run_batched(args, torch, dev, world, barrier, flush):
@@ -335,10 +340,7 @@ def run_batched(args, torch, dev, world, barrier, flush):
     p1.record(st)
     barrier()
     plain_ms = p0.elapsed_time(p1) / psteps
-    t = torch.tensor([ms, plain_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, plain_ms = float(t[0]), float(t[1])
+    ms, plain_ms = max_over_ranks([ms, plain_ms], dev)
     nas = plan.sig_np['na'].astype(np.int64)
     Ns = plan.sig_np['N'].astype(np.int64)
     tot = int(Ns.sum())
@@ -420,11 +422,8 @@ def run_train(args, torch, dev, world, barrier, flush):
         fwd(x).backward()
     ev[3].record(st)
     barrier()
-    t = torch.tensor([ev[0].elapsed_time(ev[1]) / steps, ev[2].elapsed_time(ev[3]) / steps],
-                     dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    f_ms, fb_ms = float(t[0]), float(t[1])
+    f_ms, fb_ms = max_over_ranks([ev[0].elapsed_time(ev[1]) / steps,
+                                  ev[2].elapsed_time(ev[3]) / steps], dev)
     peak = torch.cuda.max_memory_allocated(dev)
     return {
         "workload": "ssq_cwt + icwt loss, batch %d x N=%d float32 chirp mixtures, "
@@ -500,10 +499,7 @@ def run_long(args, torch, dev, world, barrier):
     fb_ms, fb_mem = timed(fwd_bwd, steps)
     del Ty
     torch.cuda.empty_cache()
-    t = torch.tensor([p_ms, b_ms, fb_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    p_ms, b_ms, fb_ms = (float(v) for v in t)
+    p_ms, b_ms, fb_ms = max_over_ranks([p_ms, b_ms, fb_ms], dev)
     hbm, src = peaks()
     fwd_bytes = B * N * (4 + 16 * na)
     bwd_bytes = B * N * (8 * na + 4 + 4)
