@@ -187,6 +187,18 @@ SSQB_API int ssqb_icwt(const void* Wx, const double* row_weights, const double* 
                        double mean_weight, int B, int na, int N, int precision,
                        void* x, void* stream);
 
+/* Inverse synchrosqueeze (issq_cwt, _ssq_cwt.py:313-400; issq_stft,
+ * _ssq_stft.py:139-198): Tx (nrows, N) complex; with K = 0, x (N) =
+ * scale * sum_k Re Tx[k, :]; with K components (K <= 16), cc and cw (N, K)
+ * int32 (device) give per column the row range [clip(cc - cw), clip(cc + cw)]
+ * (clipped to [0, nrows], empty where cc = -1) and x (K + 1, N) float64
+ * holds each component's range sum and, last, the sum of the rows outside
+ * every range, all times scale. With K = 0, x has the real type of the
+ * precision. scale = 2 / Css for the CWT, 2 / window[n_fft / 2] for
+ * the STFT. Float64 accumulation. */
+SSQB_API int ssqb_issq(const void* Tx, int nrows, int N, const int32_t* cc, const int32_t* cw,
+                       int K, double scale, int precision, void* x, void* stream);
+
 /* ---- batches of signals of uneven length ---------------------------------
  * ssqueezepy transforms a 2D input of equal-length rows (_cwt.py:270-271) and
  * squeezes it one signal at a time (ssqueezing.py:210-214); signals of

@@ -413,3 +413,31 @@ def stft_adjoint(gS, window, n_fft, N, hop=1, padtype='reflect', modulated=True)
         keep = src >= 0
         np.add.at(out[b], src[keep], gxp[keep])
     return out.reshape(gS.shape[:-2] + (N,))
+
+
+#### inverse synchrosqueezing (_ssq_cwt.py:313-400, _ssq_stft.py:139-198) ####
+def issq(Tx, scale, cc=None, cw=None):
+    """scale * sum_k Re Tx[k] (full inversion) or, with curve centres `cc` and
+    widths `cw` (N, K), the K components summed over their row bands
+    [clip(cc - cw), clip(cc + cw)] (empty where cc = -1) and, last, the rows
+    outside every band: (K + 1, N) float64."""
+    Tx = np.asarray(Tx)
+    if cc is None and cw is None:
+        return Tx.real.sum(axis=0) * scale
+    cc = np.asarray(cc).reshape(len(cc), -1).astype(np.int32)
+    cw = np.asarray(cw).reshape(len(cw), -1).astype(np.int32)
+    nr, N = Tx.shape
+    K = cc.shape[1]
+    x = np.zeros((K + 1, N))
+    keep = np.ones(Tx.shape, bool)
+    for n in range(K):
+        up = np.clip(cc[:, n] + cw[:, n], 0, nr)
+        lo = np.clip(cc[:, n] - cw[:, n], 0, nr)
+        up[cc[:, n] == -1] = 0
+        lo[cc[:, n] == -1] = 1
+        rows = np.arange(nr)[:, None]
+        band = (rows >= lo[None, :]) & (rows <= up[None, :])
+        x[n] = np.where(band, Tx.real, 0).sum(axis=0)
+        keep &= ~band
+    x[K] = np.where(keep, Tx.real, 0).sum(axis=0)
+    return x * scale

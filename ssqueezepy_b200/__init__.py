@@ -8,7 +8,8 @@ include/ssqb.h). Host code only derives float64 parameters (scales,
 frequencies, bin mapping); there is no CPU fallback.
 """
 from ._transforms import (cwt, ssq_cwt, icwt, stft, ssq_stft, ssqueeze,
-                          phase_cwt, phase_stft, Wavelet, configure)
+                          phase_cwt, phase_stft, issq_cwt, issq_stft, Wavelet,
+                          configure)
 from ._params import (p2up, process_scales, make_scales, cwt_scalebounds,
                       center_frequency, adm_ssq, logscale_transition_idx,
                       infer_scaletype, nv_from_scales)
@@ -20,7 +21,7 @@ __all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
            'phase_cwt', 'phase_stft', 'Wavelet', 'configure', 'p2up', 'process_scales',
            'make_scales', 'cwt_scalebounds', 'center_frequency', 'adm_ssq',
            'logscale_transition_idx', 'infer_scaletype', 'nv_from_scales',
-           'SsqCwtBatch', 'ssq_cwt_batch']
+           'SsqCwtBatch', 'ssq_cwt_batch', 'issq_cwt', 'issq_stft']
 
 
 def wavs():

@@ -11,6 +11,7 @@ arrays or torch tensors (CPU or CUDA); outputs are CUDA tensors
 (`astensor=True`, the default) or numpy arrays.
 """
 import os
+import warnings
 
 import numpy as np
 import torch
@@ -20,7 +21,7 @@ from . import _lib as L
 from . import _params as P
 
 __all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
-           'phase_cwt', 'phase_stft', 'Wavelet', 'configure']
+           'phase_cwt', 'phase_stft', 'issq_cwt', 'issq_stft', 'Wavelet', 'configure']
 
 Wavelet = P.Wavelet
 
@@ -477,6 +478,77 @@ def _icwt_weights(scales, scaletype, Cpsi, l1_norm):
         norm = scales if l1_norm else scales**1.5
         c = (2 / Cpsi) * np.pi / 4
     return c / norm, 1.0
+
+
+#### inverse synchrosqueezing #################################################
+def issq_cwt(Tx, wavelet='gmw', cc=None, cw=None):
+    """Inverse synchrosqueezed CWT (_ssq_cwt.py:313-363): x = (2/Css) sum_k
+    Re Tx[k]; with curve centres `cc` and widths `cw` (N, K), the K
+    components over their row bands and the remainder, (K + 1, N) float64.
+    Same container kind as `Tx`."""
+    wavelet = P.Wavelet._init_if_not_isinstance(wavelet)
+    return _issq(Tx, cc, cw, 2 / P.adm_ssq(wavelet))
+
+
+def issq_stft(Tx, window=None, cc=None, cw=None, n_fft=None, win_len=None,
+              hop_len=1, modulated=True):
+    """Inverse synchrosqueezed STFT (_ssq_stft.py:139-198): as `issq_cwt`
+    with the scale 2 / window[n_fft // 2]."""
+    if not modulated:
+        raise ValueError("inversion with `modulated == False` is unsupported.")
+    if hop_len != 1:
+        raise ValueError("inversion with `hop_len != 1` is unsupported.")
+    n_fft = n_fft or (Tx.shape[0] - 1) * 2
+    win_len = win_len or n_fft
+    window, _ = P.get_window(window, win_len, n_fft=n_fft)
+    _check_nola(window, hop_len)
+    if abs(np.argmax(window) - len(window) // 2) > 1:
+        warnings.warn("`window` maximum not centered; results may be inaccurate.")
+    return _issq(Tx, cc, cw, 2 / window[len(window) // 2])
+
+
+def _check_nola(window, hop_len):
+    """Warnings of _stft.py:313-320 (non-zero overlap-add)."""
+    from scipy import signal as sig
+    if hop_len > len(window):
+        warnings.warn("`hop_len > len(window)`; STFT not invertible")
+    elif not sig.check_NOLA(window, len(window), len(window) - hop_len):
+        warnings.warn("`window` fails Non-zero Overlap Add (NOLA) criterion; "
+                      "STFT not invertible")
+
+
+def _issq(Tx, cc, cw, scale):
+    is_np = isinstance(Tx, np.ndarray)
+    T = torch.as_tensor(Tx)
+    if not T.is_complex():
+        raise ValueError("`Tx` must be complex")
+    if T.ndim != 2:
+        raise ValueError("`Tx` must be 2D (rows, time) (got ndim=%s)" % T.ndim)
+    L.require_cuda()
+    dev = _device_of(Tx)
+    T = T.to(dev).contiguous()
+    nrows, N = T.shape
+    prec = L.F64 if T.dtype == torch.complex128 else L.F32
+    if cc is None and cw is None:
+        K, ccd, cwd = 0, None, None
+        out = torch.empty(N, dtype=torch.float64 if prec else torch.float32, device=dev)
+    else:
+        cc = np.asarray(P._to_numpy(cc))
+        cw = np.asarray(P._to_numpy(cw))
+        cc = (cc.reshape(-1, 1) if cc.ndim == 1 else cc).astype(np.int32)
+        cw = (cw.reshape(-1, 1) if cw.ndim == 1 else cw).astype(np.int32)
+        if cc.shape != cw.shape or cc.shape[0] != N:
+            raise ValueError("`cc` and `cw` must both be (%d, K) (got %s, %s)"
+                             % (N, cc.shape, cw.shape))
+        K = cc.shape[1]
+        ccd = torch.as_tensor(np.ascontiguousarray(cc), device=dev)
+        cwd = torch.as_tensor(np.ascontiguousarray(cw), device=dev)
+        out = torch.empty((K + 1, N), dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        rc = L.load().ssqb_issq(L.ptr(T), nrows, N, L.ptr(ccd), L.ptr(cwd), K,
+                                float(scale), prec, L.ptr(out), L.stream_ptr())
+    L.check(rc, 'issq')
+    return out.cpu().numpy() if is_np else out
 
 
 #### squeeze on existing transforms ##########################################

@@ -465,6 +465,20 @@ int ssqb_icwt(const void* Wx, const double* row_weights, const double* x_mean,
   return SSQB_OK;
 }
 
+int ssqb_issq(const void* Tx, int nrows, int N, const int32_t* cc, const int32_t* cw, int K,
+              double scale, int precision, void* x, void* stream) {
+  if (!Tx || !x) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (nrows < 1 || N < 1) return fail(SSQB_EINVAL, "nrows and N must be >= 1");
+  if (K < 0 || K > 16) return fail(SSQB_EUNSUPPORTED, "K must be in [0, 16]");
+  if (K > 0 && (!cc || !cw)) return fail(SSQB_EINVAL, "components need cc and cw");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  const int e = run_issq(Tx, nrows, N, cc, cw, K, scale, data_prec(precision), x,
+                         (cudaStream_t)stream);
+  if (e) return cuda_fail((cudaError_t)e, "issq launch");
+  return SSQB_OK;
+}
+
 int ssqb_cwt_noalloc(const void* x, int B, int N, int Npad, int n1, int padtype,
                      int rpadded, const double* scales, int na,
                      const ssqb_wavelet* wavelet, double dt, const ssqb_bins* bins,

@@ -123,4 +123,63 @@ int run_icwt(const void* Wx, const double* w, const double* x_mean, double mean_
   return cudaGetLastError();
 }
 
+// Inverse synchrosqueeze (_ssq_cwt.py:366-400): for column j, component n
+// sums Re Tx[k, j] over rows k in [lo, hi] with hi = clip(cc + cw, 0, nrows),
+// lo = clip(cc - cw, 0, nrows) (an empty range where cc = -1); the last
+// output row sums the rows outside every component's range. K = 0: the sum
+// of all rows. Rows ascending, float64 accumulation, times `scale`.
+constexpr int kMaxIssqComponents = 16;
+
+template <typename C>
+__global__ void issq_kernel(const C* __restrict__ Tx, int nrows, int N,
+                            const int* __restrict__ cc, const int* __restrict__ cw, int K,
+                            double scale, void* __restrict__ xv) {
+  typedef typename RealOf<C>::type T;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  int lo[kMaxIssqComponents], hi[kMaxIssqComponents];
+  double part[kMaxIssqComponents];
+  for (int n = 0; n < K; ++n) {
+    const long long c = cc[(size_t)j * K + n], w = cw[(size_t)j * K + n];
+    long long up = c + w, dn = c - w;
+    up = up < 0 ? 0 : (up > nrows ? nrows : up);
+    dn = dn < 0 ? 0 : (dn > nrows ? nrows : dn);
+    if (c == -1) { up = 0; dn = 1; }
+    lo[n] = (int)dn;
+    hi[n] = (int)up;
+    part[n] = 0.0;
+  }
+  double rest = 0.0;
+  for (int k = 0; k < nrows; ++k) {
+    const double v = (double)Tx[(size_t)k * N + j].x;
+    bool in = false;
+    for (int n = 0; n < K; ++n) {
+      if (k >= lo[n] && k <= hi[n]) {
+        part[n] += v;
+        in = true;
+      }
+    }
+    if (!in) rest += v;
+  }
+  if (K > 0) {  // components: float64 rows, as the reference's np.zeros((K + 1, N))
+    double* x = (double*)xv;
+    for (int n = 0; n < K; ++n) x[(size_t)n * N + j] = part[n] * scale;
+    x[(size_t)K * N + j] = rest * scale;
+  } else {
+    ((T*)xv)[j] = (T)(rest * scale);
+  }
+}
+
+int run_issq(const void* Tx, int nrows, int N, const int* cc, const int* cw, int K,
+             double scale, int precision, void* x, cudaStream_t st) {
+  const dim3 grid((N + 255) / 256);
+  if (precision == 0)
+    issq_kernel<float2><<<grid, 256, 0, st>>>((const float2*)Tx, nrows, N, cc, cw, K, scale,
+                                              x);
+  else
+    issq_kernel<double2><<<grid, 256, 0, st>>>((const double2*)Tx, nrows, N, cc, cw, K, scale,
+                                               x);
+  return cudaGetLastError();
+}
+
 }  // namespace ssqb

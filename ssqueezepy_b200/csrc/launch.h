@@ -91,6 +91,8 @@ int run_squeeze_f64(const double2* Wx, int src_kind, const void* src, int idx_pi
 
 int run_icwt(const void* Wx, const double* w, const double* x_mean, double mean_weight,
              int B, int na, int N, int precision, void* x, cudaStream_t st);
+int run_issq(const void* Tx, int nrows, int N, const int* cc, const int* cw, int K,
+             double scale, int precision, void* x, cudaStream_t st);
 
 // count launches of this host thread into *c instead of launching (NULL:
 // launch again)

@@ -200,6 +200,27 @@ tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_
   C* zrow = Z + (size_t(blockIdx.z) * rows_in_tile + blockIdx.y) * NARR * L;
   typedef decltype(op.bind(0)) BOp;
   const auto ld = make_p1_loader<BOp, C, NARR>(bop, b, row, k1_0, L1);
+  if constexpr (HasGather<P1Loader<BOp, C, NARR>>::value) {
+    // A band narrower than L1 bins leaves whole columns k1 without inputs
+    // (column k1 holds the bins k = k1 mod L1). If none of this CTA's
+    // columns meets the band, its transforms are exactly zero.
+    const int W = ld.khi - ld.klo + 1;
+    if (W < L1) {
+      const int r0 = ((ld.klo % L1) + L1) % L1;
+      bool any = false;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) any |= ((k1_0 + f - r0 + L1) % L1) < W;
+      if (!any) {
+        const C zero = mk((typename RealOf<C>::type)0, (typename RealOf<C>::type)0);
+        for (int e = threadIdx.x; e < NF * L2; e += kNT) {
+          const size_t o = (size_t)(e / NF) * L1 + k1_0 + (e % NF);
+#pragma unroll
+          for (int a = 0; a < NARR; ++a) zrow[a * L + o] = zero;
+        }
+        return;
+      }
+    }
+  }
   Pass1Store<C, NARR, SIGN> st{tb, zrow, k1_0, L1, log2L};
   fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }

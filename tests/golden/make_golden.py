@@ -15,6 +15,10 @@ Writes:
   digests.npz      full-size (N=10,000 and N=160,000) float64 digests: row
                    norms and row sums of Wx and Tx, total norms, and a bin
                    histogram, for size-independent checks
+  issq.npz         issq_cwt / issq_stft of seeded complex Tx (rebuilt from
+                   the seed by the tests), full and per-component inversion
+
+`--only issq` writes issq.npz alone.
 """
 import os
 import sys
@@ -184,5 +188,38 @@ def main(ref_root):
     np.savez_compressed(os.path.join(HERE, 'digests.npz'), **dg)
 
 
+def issq_inputs():
+    """Seeded complex Tx (CWT-like 120 x 700, STFT-like 129 x 700) and curve
+    centres / widths (700, 2) with some columns marked -1 (no curve)."""
+    rng = np.random.default_rng(77)
+    Tc = rng.standard_normal((120, 700)) + 1j * rng.standard_normal((120, 700))
+    Ts = rng.standard_normal((129, 700)) + 1j * rng.standard_normal((129, 700))
+    cc = rng.integers(0, 120, (700, 2))
+    cc[rng.random((700, 2)) < 0.1] = -1
+    cw = rng.integers(0, 12, (700, 2))
+    return Tc, Ts, cc, cw
+
+
+def issq_fixtures(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    Tc, Ts, cc, cw = issq_inputs()
+    out = {}
+    for key, (name, opts) in (('gmw', ('gmw', {})), ('morlet6', ('morlet', {'mu': 6.}))):
+        w = sq.Wavelet((name, dict(opts, dtype='float64')))  # float64 admissibility
+        out['cwt_full_' + key] = sq.issq_cwt(Tc, w)
+        out['cwt_comp_' + key] = sq.issq_cwt(Tc, w, cc, cw)
+    out['stft_full_hann256'] = sq.issq_stft(Ts, 'hann', n_fft=256)
+    out['stft_comp_hann256'] = sq.issq_stft(Ts, 'hann', cc=cc, cw=cw, n_fft=256)
+    np.savez_compressed(os.path.join(HERE, 'issq.npz'), **out)
+
+
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    args = [a for a in sys.argv[1:] if not a.startswith('--')]
+    root = args[0] if args else '/root/reference'
+    if '--only' in sys.argv and 'issq' in sys.argv:
+        issq_fixtures(root)
+    else:
+        main(root)
+        issq_fixtures(root)

@@ -1,6 +1,8 @@
 # -*- coding: utf-8 -*-
 """Pin the float64 oracle (oracle/ssq_oracle.py) against ssqueezepy's own
 float64 outputs stored in tests/golden/ (generated by make_golden.py)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -146,3 +148,26 @@ def test_stft_adjoint_is_the_transpose(padtype, hop):
     gx = O.stft_adjoint(g, win, n_fft, N, hop=hop, padtype=padtype)
     lhs = np.real(np.vdot(g, Sx))
     assert abs(lhs - float(x @ gx)) <= 1e-10 * np.abs(g).sum() * np.abs(Sx).max()
+
+
+def _issq_inputs():
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        'make_golden', os.path.join(os.path.dirname(__file__), 'golden', 'make_golden.py'))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.issq_inputs()
+
+
+def test_oracle_issq_matches_golden():
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'issq.npz'))
+    Tc, Ts, cc, cw = _issq_inputs()
+    for key, wav in (('gmw', ('gmw', {})), ('morlet6', ('morlet', {'mu': 6.}))):
+        scale = 2 / P.adm_ssq(P.Wavelet(wav))
+        assert rel_l2(O.issq(Tc, scale), g['cwt_full_' + key]) < 1e-12
+        assert rel_l2(O.issq(Tc, scale, cc, cw), g['cwt_comp_' + key]) < 1e-12
+    win, _ = P.get_window('hann', 256, n_fft=256)
+    scale = 2 / win[128]
+    assert rel_l2(O.issq(Ts, scale), g['stft_full_hann256']) < 1e-12
+    assert rel_l2(O.issq(Ts, scale, cc, cw), g['stft_comp_hann256']) < 1e-12
