@@ -57,9 +57,9 @@ def test_issq_matches_reference(dtype):
 
 @pytest.mark.gpu
 def test_issq_cwt_reconstructs_the_signal():
-    """ssq_cwt then issq_cwt gives back x up to the transform's own
-    reconstruction error (the reference's test bound for GMW,
-    reconstruction_test.py: relative error well under 10 %)."""
+    """ssq_cwt then issq_cwt gives back x up to the synchrosqueezing's own
+    reconstruction error (4.3e-3 relative L2 for this signal in the float64
+    oracle)."""
     import torch
     if not torch.cuda.is_available():
         pytest.skip('no CUDA device')
@@ -68,4 +68,4 @@ def test_issq_cwt_reconstructs_the_signal():
     x = S.chirp_tone(4096, seed=2)
     Tx, *_ = sb.ssq_cwt(x, ('gmw', {'dtype': 'float64'}), astensor=False)
     xr = sb.issq_cwt(Tx, ('gmw', {'dtype': 'float64'}))
-    assert np.linalg.norm(xr - x) / np.linalg.norm(x) < 0.1
+    assert np.linalg.norm(xr - x) / np.linalg.norm(x) < 0.02  # 4.3e-3 in the oracle
