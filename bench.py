@@ -43,6 +43,9 @@ UNIT = "signal-samples/s"
 N_SIG = 160000
 WAVELET = ('gmw', {'gamma': 3., 'beta': 60., 'dtype': 'float32'})
 L2_BYTES = 126 * 2**20
+# DRAM bytes the fused CWT call moves per (row, sample), from the ncu capture
+# summarised in profiles/traffic_ssq_cwt_N40000_gmw.md
+CWT_TRAFFIC_PER_ROW_SAMPLE = 15.73
 
 
 def chirp_signal(N, seed=0):
@@ -546,7 +549,12 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
             "stages_ms": {"cwt": cwt_avg, "squeeze": sq_avg},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": None, "peak_source": src,
+                         "traffic": (CWT_TRAFFIC_PER_ROW_SAMPLE * na * N
+                                     if dom == 'cwt' else None),
+                         "traffic_source": "ncu dram__bytes_read+write of the fused CWT "
+                                           "call at N=40,000 (277 rows), 15.73 B per "
+                                           "(row, sample), scaled to this call",
+                         "peak_source": src,
                          "path_frac": alg_total / (step_ms_max * 1e-3) / 1e9 / hbm},
             "e2e": (None if e2e_value is None else
                     {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * N,

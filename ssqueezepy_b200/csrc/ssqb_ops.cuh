@@ -304,11 +304,20 @@ struct CwtOp {
   __device__ void load(int b, int row, int k, C (&v)[2]) const {
     finish(b, row, k, __ldg(xh + (size_t)b * Npad + k), v);
   }
-  __device__ void finish(int, int row, int k, double2 xv, C (&v)[2]) const {
+  __device__ void finish(int b, int row, int k, double2 xv, C (&v)[2]) const {
+    apply(k, xv, psi(row, k), v);
+  }
+  // psih(scale * xi_k) with the Nyquist bin halved (wavelets.py:86-95)
+  __device__ double psi(int row, int k) const {
     const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
     const double xi = (double)kk * h;
     double ps = psih_fp64(wav, scales[row] * xi);
-    if (k == (Npad >> 1)) ps *= 0.5;  // Nyquist bin halved (wavelets.py:86-95)
+    if (k == (Npad >> 1)) ps *= 0.5;
+    return ps;
+  }
+  __device__ void apply(int k, double2 xv, double ps, C (&v)[2]) const {
+    const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
+    const double xi = (double)kk * h;
     const double2 y = make_double2(ps * xv.x, ps * xv.y);
     const double c = xi * inv_dt;
     v[0] = to_c<C>(y);

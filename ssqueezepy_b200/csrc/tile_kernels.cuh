@@ -114,8 +114,25 @@ struct P1Loader<BOp, C, NARR, std::enable_if_t<BOp::kSplitLoad>> {
     double2 raw[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) raw[r] = op.raw(b, k1_0 + f + L1 * (j + r * stride), klo, khi);
+    if constexpr (std::is_same<C, float2>::value) {
+      // float32 transforms: one copy of the wavelet code (rolled loop) keeps
+      // the kernel small enough for the instruction cache (measured faster;
+      // with float64 transforms the unrolled form is faster)
+      double ps[R];
+#pragma unroll 1
+      for (int r = 0; r < R; ++r) {
+        const int k = k1_0 + f + L1 * (j + r * stride);
+        const int kk = (k <= (op.Npad >> 1)) ? k : k - op.Npad;
+        ps[r] = (kk >= klo && kk <= khi) ? op.psi(row, k) : 0.0;
+      }
 #pragma unroll
-    for (int r = 0; r < R; ++r) op.finish(b, row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
+      for (int r = 0; r < R; ++r)
+        op.apply(k1_0 + f + L1 * (j + r * stride), raw[r], ps[r], t[r]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        op.finish(b, row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
+    }
   }
 };
 
