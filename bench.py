@@ -15,7 +15,8 @@ Further legs, each a key of the same line:
   long     8 x N=1,048,576, GMW, 'log:maximal' (613 rows): plain forward,
            batched forward, forward + backward, peak memory;
   fwd_bwd  64 x N=16,384 Morlet: loss MSE(|Tx(x)|,|Tx(y)|) + MSE(icwt(Wx), y),
-           forward vs forward + backward through the adjoint kernels.
+           forward vs forward + backward through the adjoint kernels;
+  stft     ssq_stft of the headline signal, Hann 512, n_fft 512, hop 1.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -262,6 +263,9 @@ def run_ours(args):
     if not args.no_batch:
         del Wx, Tx, idx, ws
         batched = run_batched(args, torch, dev, world, barrier, flush)
+    stft_ = None
+    if not args.no_stft:
+        stft_ = run_stft(args, torch, dev, world, barrier, flush)
     long_ = None
     if not args.no_long:
         torch.cuda.empty_cache()
@@ -273,7 +277,8 @@ def run_ours(args):
     clocks = clk.stop() if clk else None
     if rank == 0:
         emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
-             launches, clocks, sc, f, const, Tx_keep, Wx_keep, batched, train, long_)
+             launches, clocks, sc, f, const, Tx_keep, Wx_keep, batched, train, long_,
+             stft_)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -439,6 +444,38 @@ def run_train(args, torch, dev, world, barrier, flush):
     }
 
 
+def run_stft(args, torch, dev, world, barrier, flush):
+    """ssq_stft of the headline signal (N = 160,000): Hann window of 512,
+    n_fft = 512, hop 1 (257 x N), through the public API with x resident on
+    the device; float32 data, float64 arithmetic."""
+    import ssqueezepy_b200 as sb
+    rank = int(os.environ.get('RANK', 0))
+    N = args.n
+    x = torch.as_tensor(chirp_signal(N, seed=rank).astype(np.float32), device=dev)
+    st = torch.cuda.current_stream()
+    for _ in range(max(args.warmup, 3)):
+        sb.ssq_stft(x, 'hann', n_fft=512)
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for e in evs:
+        flush.zero_()
+        e[0].record(st)
+        sb.ssq_stft(x, 'hann', n_fft=512)
+        e[1].record(st)
+    barrier()
+    ms, = max_over_ranks([float(np.mean([a.elapsed_time(b) for a, b in evs]))], dev)
+    hbm, src = peaks()
+    alg = (4 + 16 * 257) * N
+    return {"workload": "ssq_stft N=%d, Hann 512, n_fft 512, hop 1 (257 rows), float32, "
+                        "reflect" % N,
+            "value": world * N / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": hbm,
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / hbm,
+                         "peak_source": src,
+                         "bytes": "N (4 + 16 * 257): read x, write Sx and Tx"}}
+
+
 def run_long(args, torch, dev, world, barrier):
     """Long signals: 8 float32 chirp mixtures of N = 1,048,576 (Npad 2,097,152),
     GMW(3,60), scales='log:maximal' (613 rows). Plain forward (one signal per
@@ -524,7 +561,8 @@ def run_long(args, torch, dev, world, barrier):
 
 
 def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
-         launches, clocks, sc, f, const, Tg, Wg, batched=None, train=None, long_=None):
+         launches, clocks, sc, f, const, Tg, Wg, batched=None, train=None, long_=None,
+         stft_=None):
     hbm, src = peaks()
     if True:
         alg_cwt = (4 + 8 * na) * N          # read x, write Wx
@@ -568,6 +606,8 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
             line["fwd_bwd"] = train
         if long_ is not None:
             line["long"] = long_
+        if stft_ is not None:
+            line["stft"] = stft_
         if world == 1 and not args.no_cpu:
             t0 = time.perf_counter()
             To, Wo, _ = oracle_step(chirp_signal(N, seed=0), sc, f, const)
@@ -598,6 +638,8 @@ def main():
                     help='skip the batched uneven-length leg')
     ap.add_argument('--batch', type=int, default=256,
                     help='signals in the batched leg (default 256)')
+    ap.add_argument('--no-stft', action='store_true',
+                    help='skip the ssq_stft leg')
     ap.add_argument('--no-long', action='store_true',
                     help='skip the 8 x 1,048,576 long-signal leg')
     ap.add_argument('--no-train', action='store_true',
