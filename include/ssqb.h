@@ -199,6 +199,23 @@ SSQB_API int ssqb_icwt(const void* Wx, const double* row_weights, const double* 
 SSQB_API int ssqb_issq(const void* Tx, int nrows, int N, const int32_t* cc, const int32_t* cw,
                        int K, double scale, int precision, void* x, void* stream);
 
+/* Time-frequency ridge extraction (ridge_extraction.py:11-232, its serial
+ * code path): Tf (nf, N) complex; s (nf) the frequency axis the jump
+ * penalty uses (log scales for the CWT, frequencies for the STFT) and
+ * scales (nf) the values reported per ridge, both of the precision's real
+ * type (device); penalty, eps and the arithmetic in that type (float32 for
+ * SSQB_F32 / SSQB_F32X). For each of n_ridges ridges: E = -log(|Tf|^2 /
+ * column max + eps), forward accumulation of min(E + penalty * ds^2) over
+ * time, backward re-tracking within eps, then rows [r - bw, r + bw) of
+ * the energy (Python slice rules) are cleared. Outputs (N, n_ridges):
+ * ridge_idx int32, ridge_f and ridge_e (real, optional). */
+SSQB_API size_t ssqb_ridges_workspace_bytes(int nf, int N, int precision);
+SSQB_API int ssqb_extract_ridges(const void* Tf, int nf, int N, const void* s,
+                                 const void* scales, double penalty, int n_ridges, int bw,
+                                 double eps, int precision, int32_t* ridge_idx, void* ridge_f,
+                                 void* ridge_e, void* workspace, size_t workspace_bytes,
+                                 void* stream);
+
 /* ---- batches of signals of uneven length ---------------------------------
  * ssqueezepy transforms a 2D input of equal-length rows (_cwt.py:270-271) and
  * squeezes it one signal at a time (ssqueezing.py:210-214); signals of

@@ -441,3 +441,40 @@ def issq(Tx, scale, cc=None, cw=None):
         keep &= ~band
     x[K] = np.where(keep, Tx.real, 0).sum(axis=0)
     return x * scale
+
+
+#### ridge extraction (ridge_extraction.py:11-232, serial code path) ##########
+def extract_ridges(Tf, scales, penalty=2., n_ridges=1, bw=15, transform='cwt'):
+    """(ridge_idxs, ridge_f, ridge_e), each (N, n_ridges): forward-backward
+    tracking of min accumulated -log normalised energy plus
+    penalty * (s_f - s_f')^2 jumps (s = log scales for 'cwt'), in the
+    arithmetic type of Tf (float32 for complex64)."""
+    Tf = np.asarray(Tf)
+    dt = np.float64 if Tf.dtype == np.complex128 else np.float32
+    eps = dt(EPS64 if dt == np.float64 else EPS32)
+    scales = np.asarray(scales, dt)
+    penalty = dt(penalty)
+    s = (np.log(scales) if transform == 'cwt' else scales).squeeze()
+    P = penalty * np.subtract.outer(s, s) ** 2
+    energy = np.abs(Tf) ** 2
+    nf, N = energy.shape
+    idxs = np.zeros((N, n_ridges), int)
+    rf = np.zeros((N, n_ridges), dt)
+    re = np.zeros((N, n_ridges), dt)
+    for i in range(n_ridges):
+        E = -np.log(energy / energy.max(axis=0) + eps)
+        pen = E.copy()
+        for t in range(1, N):
+            pen[:, t] += np.amin(pen[:, t - 1][None, :] + P, axis=1)
+        r = np.argmin(pen, axis=0)
+        for t in range(N - 2, -1, -1):
+            val = pen[r[t + 1], t + 1] - E[r[t + 1], t + 1]
+            hit = np.nonzero(np.abs(val - (pen[:, t] + P[r[t + 1], :])) < eps)[0]
+            if len(hit):
+                r[t] = hit[-1]
+        idxs[:, i] = r
+        rf[:, i] = scales[r]
+        re[:, i] = energy[r, np.arange(N)]
+        for t in range(N):
+            energy[int(r[t] - bw):int(r[t] + bw), t] = 0
+    return idxs, rf, re

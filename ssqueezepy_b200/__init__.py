@@ -14,6 +14,7 @@ from ._params import (p2up, process_scales, make_scales, cwt_scalebounds,
                       center_frequency, adm_ssq, logscale_transition_idx,
                       infer_scaletype, nv_from_scales)
 from ._batch import SsqCwtBatch, ssq_cwt_batch
+from ._ridges import extract_ridges
 from . import _lib
 
 __version__ = '0.1.0'
@@ -21,7 +22,7 @@ __all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'ssq_stft', 'ssqueeze',
            'phase_cwt', 'phase_stft', 'Wavelet', 'configure', 'p2up', 'process_scales',
            'make_scales', 'cwt_scalebounds', 'center_frequency', 'adm_ssq',
            'logscale_transition_idx', 'infer_scaletype', 'nv_from_scales',
-           'SsqCwtBatch', 'ssq_cwt_batch', 'issq_cwt', 'issq_stft']
+           'SsqCwtBatch', 'ssq_cwt_batch', 'issq_cwt', 'issq_stft', 'extract_ridges']
 
 
 def wavs():

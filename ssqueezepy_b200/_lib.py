@@ -53,6 +53,9 @@ SIGNATURES = {
                               ctypes.POINTER(CWavelet), _d, ctypes.POINTER(CBins), _d,
                               _i, _vp, _vp, _vp, _vp, _i, _vp]),
     'ssqb_cwt_noalloc_max_bytes': (_sz, []),
+    'ssqb_ridges_workspace_bytes': (_sz, [_i, _i, _i]),
+    'ssqb_extract_ridges': (_i, [_vp, _i, _i, _vp, _vp, _d, _i, _i, _d, _i, _vp, _vp, _vp, _vp,
+                                 _sz, _vp]),
     'ssqb_issq': (_i, [_vp, _i, _i, _vp, _vp, _i, _d, _i, _vp, _vp]),
     'ssqb_cwt_batch_workspace_bytes': (_sz, [_i, _i, _i]),
     'ssqb_cwt_batch': (_i, [_vp, _vp, _vp, _i, _i, _i, ctypes.POINTER(CWavelet), _d, _d,

@@ -479,6 +479,33 @@ int ssqb_issq(const void* Tx, int nrows, int N, const int32_t* cc, const int32_t
   return SSQB_OK;
 }
 
+size_t ssqb_ridges_workspace_bytes(int nf, int N, int precision) {
+  if (nf < 1 || N < 1 || !valid_precision(precision)) return 0;
+  return ridges_workspace(nf, N, data_prec(precision) == SSQB_F64);
+}
+
+int ssqb_extract_ridges(const void* Tf, int nf, int N, const void* s, const void* scales,
+                        double penalty, int n_ridges, int bw, double eps, int precision,
+                        int32_t* ridge_idx, void* ridge_f, void* ridge_e, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  if (!Tf || !s || !scales || !ridge_idx || !workspace)
+    return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (nf < 1 || N < 1 || n_ridges < 1) return fail(SSQB_EINVAL, "nf, N, n_ridges must be >= 1");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  const bool f64 = data_prec(precision) == SSQB_F64;
+  if (2 * (size_t)nf * (f64 ? 8 : 4) > 227 * 1024)
+    return fail(SSQB_EUNSUPPORTED, "too many frequency rows for the shared-memory sweep");
+  const size_t need = ridges_workspace(nf, N, f64);
+  if (workspace_bytes < need)
+    return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                     " bytes");
+  const int e = run_ridges(Tf, nf, N, s, scales, penalty, n_ridges, bw, eps, f64, ridge_idx,
+                           ridge_f, ridge_e, workspace, (cudaStream_t)stream);
+  if (e) return cuda_fail((cudaError_t)e, "ridge launch");
+  return SSQB_OK;
+}
+
 int ssqb_cwt_noalloc(const void* x, int B, int N, int Npad, int n1, int padtype,
                      int rpadded, const double* scales, int na,
                      const ssqb_wavelet* wavelet, double dt, const ssqb_bins* bins,

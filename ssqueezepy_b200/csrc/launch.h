@@ -111,6 +111,12 @@ int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* 
                           int nsig, int max_na, int max_N, float2* Tx, int* status,
                           cudaStream_t st);
 
+// ridge extraction (k_ridges.cu)
+size_t ridges_workspace(int nf, int N, bool f64);
+int run_ridges(const void* Tf, int nf, int N, const void* s, const void* scales, double penalty,
+               int n_ridges, int bw, double eps, bool f64, int* idx_out, void* f_out,
+               void* e_out, void* ws, cudaStream_t st);
+
 // adjoints (reverse-mode differentiation)
 constexpr size_t kAdjChunkBytes = (size_t)64 << 20;  // row chunk: Y + Z
 size_t cwt_adjoint_workspace(int B, int Npad, int na, bool f64);

@@ -18,7 +18,11 @@ Writes:
   issq.npz         issq_cwt / issq_stft of seeded complex Tx (rebuilt from
                    the seed by the tests), full and per-component inversion
 
-`--only issq` writes issq.npz alone.
+  ridges.npz       extract_ridges (serial code path) of a seeded synthetic
+                   Tf with two ridges, float64 and float32, log and linear
+                   frequency axes, with its inputs
+
+`--only issq` / `--only ridges` writes that file alone.
 """
 import os
 import sys
@@ -215,11 +219,42 @@ def issq_fixtures(ref_root):
     np.savez_compressed(os.path.join(HERE, 'issq.npz'), **out)
 
 
+def ridges_fixtures(ref_root):
+    """Tf (64 x 400): two ridges (a rising and a falling frequency track,
+    amplitudes 1 and 0.6) over complex noise of 0.05; scales geomspace(1, 50)
+    for the log axis, linspace(0, 0.5) for the linear one."""
+    sys.path.insert(0, ref_root)
+    from ssqueezepy.ridge_extraction import extract_ridges
+    rng = np.random.default_rng(31)
+    nf, N = 64, 400
+    t = np.arange(N)
+    f = np.arange(nf)[:, None]
+    c1 = 10 + 40 * t / N
+    c2 = 55 - 30 * (t / N) ** 2
+    Tf = (np.exp(-(f - c1) ** 2 / 6) + 0.6 * np.exp(-(f - c2) ** 2 / 4)
+          + 0.05 * (rng.standard_normal((nf, N)) + 1j * rng.standard_normal((nf, N))))
+    Tf = Tf * np.exp(1j * rng.uniform(0, 2 * np.pi, (nf, N)))
+    out = dict(Tf=Tf, scales_log=np.geomspace(1, 50, nf), scales_lin=np.linspace(0, .5, nf))
+    for dt in ('f64', 'f32'):
+        T = Tf if dt == 'f64' else Tf.astype(np.complex64)
+        for ax, tr in (('log', 'cwt'), ('lin', 'stft')):
+            sc = out['scales_' + ax]
+            for nr, bw in ((1, 15), (2, 4)):
+                key = '%s_%s_r%d' % (dt, ax, nr)
+                i, fr, e = extract_ridges(T, sc, penalty=2., n_ridges=nr, bw=bw, transform=tr,
+                                          get_params=True, parallel=False)
+                out[key + '_idx'], out[key + '_f'], out[key + '_e'] = i, fr, e
+    np.savez_compressed(os.path.join(HERE, 'ridges.npz'), **out)
+
+
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
     root = args[0] if args else '/root/reference'
     if '--only' in sys.argv and 'issq' in sys.argv:
         issq_fixtures(root)
+    elif '--only' in sys.argv and 'ridges' in sys.argv:
+        ridges_fixtures(root)
     else:
         main(root)
         issq_fixtures(root)
+        ridges_fixtures(root)

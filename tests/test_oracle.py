@@ -171,3 +171,16 @@ def test_oracle_issq_matches_golden():
     scale = 2 / win[128]
     assert rel_l2(O.issq(Ts, scale), g['stft_full_hann256']) < 1e-12
     assert rel_l2(O.issq(Ts, scale, cc, cw), g['stft_comp_hann256']) < 1e-12
+
+
+def test_oracle_ridges_match_golden():
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'ridges.npz'))
+    for dt in ('f64', 'f32'):
+        T = g['Tf'] if dt == 'f64' else g['Tf'].astype(np.complex64)
+        for ax, tr in (('log', 'cwt'), ('lin', 'stft')):
+            for nr, bw in ((1, 15), (2, 4)):
+                key = '%s_%s_r%d' % (dt, ax, nr)
+                i, f, e = O.extract_ridges(T, g['scales_' + ax], 2., nr, bw, tr)
+                assert np.array_equal(i, g[key + '_idx']), key
+                assert np.array_equal(f, g[key + '_f']), key
+                assert np.allclose(e, g[key + '_e'], rtol=1e-6 if dt == 'f32' else 1e-14), key
