@@ -128,11 +128,13 @@ class Wavelet():
             if norm not in ('bandpass', 'energy'):
                 raise ValueError("`norm` must be 'energy' or 'bandpass' "
                                  f"(got '{norm}')")
-            if order != 0 or centered:
+            if centered:
                 raise NotImplementedError(
-                    "GMW `order > 0` and `centered_scale=True` are not on the "
-                    "accelerated path")
+                    "GMW `centered_scale=True` is not on the accelerated path")
+            order = _check_order(order)
             self.config = dict(gamma=gamma, beta=beta, norm=norm)
+            if order != 0:
+                self.config['order'] = order
             self.kind = (self.KIND_GMW_L1 if norm == 'bandpass' else
                          self.KIND_GMW_L2)
             if norm == 'energy':
@@ -180,6 +182,30 @@ class Wavelet():
         return self._dtype
 
     @property
+    def order(self):
+        return self.config.get('order', 0)
+
+    def poly(self):
+        """Laguerre coefficients kc of a higher-order GMW: psih = C(w) * base(w)
+        with C(w) = sum_m kc[m] (2 w^gamma)^m and base the order-0 exponential
+        without its norm constant (_gmw.py:268-296, 320-347). An order tuple
+        averages the wavelets of its orders, i.e. their coefficient vectors
+        (cwt_higher_order, _cwt.py:517-610, averages the transforms, which are
+        linear in the wavelet). None for order 0."""
+        order = self.order
+        if order == 0 or self.kind == self.KIND_MORLET:
+            return None
+        c = self.config
+        norm = c['norm']
+        if isinstance(order, tuple):
+            ks = [gmw_k_constants(c['gamma'], c['beta'], k, norm) for k in order]
+            out = np.zeros(max(len(k) for k in ks))
+            for k in ks:
+                out[:len(k)] += k
+            return out / len(ks)
+        return gmw_k_constants(c['gamma'], c['beta'], order, norm)
+
+    @property
     def name(self):
         if self.kind == self.KIND_MORLET:
             return 'Morlet'
@@ -225,6 +251,19 @@ class Wavelet():
                               - k['ks'] * np.exp(-.5 * w**2))
         nonneg = (w >= 0)
         w = w * nonneg
+        kc = self.poly()
+        if kc is not None:
+            y = 2 * w**k['gamma']
+            C = np.zeros_like(w)
+            for m in range(len(kc)):
+                C = C + kc[m] * y**m
+            with np.errstate(divide='ignore'):
+                if self.kind == self.KIND_GMW_L1:
+                    e = (-k['beta'] * k['wcl'] + k['wc']**k['gamma']
+                         + k['beta'] * np.log(w) - w**k['gamma'])
+                else:
+                    e = k['beta'] * np.log(w) - w**k['gamma']
+                return C * np.exp(e) * nonneg
         with np.errstate(divide='ignore'):
             if self.kind == self.KIND_GMW_L1:
                 return 2 * np.exp(-k['beta'] * k['wcl'] + k['wc']**k['gamma']
@@ -260,6 +299,15 @@ class Wavelet():
             neg = np.sqrt(max(0., -2 * log_floor - mu**2))
             return (min(mu - r, -neg), mu + r)
         g, b, wc = k['gamma'], k['beta'], k['wc']
+        if self.poly() is not None:
+            # a polynomial factor moves the peak: scan log|psih| on a fine
+            # log grid and widen by a grid step on each side
+            w = np.geomspace(1e-8 * wc, 1e3 * wc, 1 << 16)
+            with np.errstate(divide='ignore'):
+                lp = np.log(np.abs(self.fn(w)))
+            keep = np.nonzero(lp >= lp.max() + log_floor)[0]
+            i0, i1 = max(keep[0] - 1, 0), min(keep[-1] + 1, len(w) - 1)
+            return (float(w[i0]), float(w[i1]))
 
         def e(w):  # log of psih relative to its peak at wc
             return b * np.log(w / wc) - (w**g - wc**g)
@@ -284,6 +332,46 @@ class Wavelet():
         if self.kind == self.KIND_GMW_L1:
             return (self.kind, k['gamma'], k['beta'], k['wc'], k['wcl'])
         return (self.kind, k['gamma'], k['beta'], k['wc'], k['l2norm'])
+
+
+MAX_GMW_ORDER = 7
+
+
+def _check_order(order):
+    if isinstance(order, (list, range)):
+        order = tuple(order)
+    if isinstance(order, tuple):
+        order = tuple(int(k) for k in order)
+        if len(order) == 1:
+            order = order[0]
+    ks = order if isinstance(order, tuple) else (int(order),)
+    if any(k < 0 or k > MAX_GMW_ORDER for k in ks):
+        raise NotImplementedError("GMW orders 0..%d are on the accelerated path "
+                                  "(got %s)" % (MAX_GMW_ORDER, order))
+    return order if isinstance(order, tuple) else int(order)
+
+
+def gmw_k_constants(gamma, beta, k, norm='bandpass'):
+    """Laguerre polynomial constants times the order-k norm, float64
+    (_gmw.py:368-396): L_m = (-1)^m Gamma(k+c+1) / (Gamma(c+m+1) Gamma(k-m+1))
+    / m!, c = r - 1, r = (2 beta + 1) / gamma; times sqrt(Gamma(r) k! /
+    Gamma(k+r)) and 2 (bandpass), or sqrt(2 pi gamma 2^r k! / Gamma(k+r))
+    (energy)."""
+    from scipy.special import gammaln, gamma as gamma_fn
+    r = (2 * beta + 1) / gamma
+    c = r - 1
+    if norm == 'bandpass':
+        coeff = np.sqrt(np.exp(gammaln(r) + gammaln(k + 1) - gammaln(k + r)))
+    else:
+        coeff = np.sqrt(2 * pi * gamma * (2**r) * np.exp(gammaln(k + 1) - gammaln(k + r)))
+    L = np.zeros(k + 1)
+    for m in range(k + 1):
+        fact = np.exp(gammaln(k + c + 1) - gammaln(c + m + 1) - gammaln(k - m + 1))
+        L[m] = (-1)**m * fact / gamma_fn(m + 1)
+    kc = L * coeff
+    if norm == 'bandpass':
+        kc = kc * 2
+    return kc
 
 
 def _dtype_str(dtype):

@@ -22,7 +22,11 @@ Writes:
                    Tf with two ridges, float64 and float32, log and linear
                    frequency axes, with its inputs
 
-`--only issq` / `--only ridges` writes that file alone.
+  higher.npz       higher-order GMW transforms (float64, N=256): cwt with
+                   order=2, cwt averaged over orders (0, 1, 2), ssq_cwt with
+                   order=(0, 1), and order-1 / order-3 wavelet samples
+
+`--only issq` / `--only ridges` / `--only higher` writes that file alone.
 """
 import os
 import sys
@@ -247,6 +251,28 @@ def ridges_fixtures(ref_root):
     np.savez_compressed(os.path.join(HERE, 'ridges.npz'), **out)
 
 
+def higher_fixtures(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    from ssqueezepy import Wavelet
+    x = chirp_signal(256, seed=4)
+    out = dict(x=x)
+    w = Wavelet(('gmw', dict(dtype='float64')))
+    Wx, sc = sq.cwt(x, w, order=2, astensor=False)
+    out['cwt_o2_Wx'], out['scales'] = Wx, sc
+    Wx, _ = sq.cwt(x, w, order=(0, 1, 2), astensor=False)
+    out['cwt_avg012_Wx'] = Wx
+    Tx, Wx, f, _ = sq.ssq_cwt(x, w, order=(0, 1), astensor=False)
+    out['ssq_avg01_Tx'], out['ssq_avg01_f'] = Tx, f
+    w1 = Wavelet(('gmw', dict(order=1, dtype='float64')))
+    out['psih_w'] = np.linspace(0, 12, 257)
+    out['psih_o1'] = np.asarray(w1(out['psih_w'])).ravel()
+    w3e = Wavelet(('gmw', dict(order=3, norm='energy', dtype='float64')))
+    out['psih_o3e'] = np.asarray(w3e(out['psih_w'])).ravel()
+    np.savez_compressed(os.path.join(HERE, 'higher.npz'), **out)
+
+
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
     root = args[0] if args else '/root/reference'
@@ -254,7 +280,10 @@ if __name__ == '__main__':
         issq_fixtures(root)
     elif '--only' in sys.argv and 'ridges' in sys.argv:
         ridges_fixtures(root)
+    elif '--only' in sys.argv and 'higher' in sys.argv:
+        higher_fixtures(root)
     else:
         main(root)
         issq_fixtures(root)
         ridges_fixtures(root)
+        higher_fixtures(root)
