@@ -201,8 +201,7 @@ def run_ours(args):
     ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     sc_d = torch.as_tensor(sc, dtype=torch.float64, device=dev)
     cst_d = torch.as_tensor(const, dtype=torch.float64, device=dev)
-    kind, *wp = w.kernel_params()
-    cw = L.make_wavelet(kind, wp, w.band())
+    cw = L.wavelet_struct(w)
     mode, bp = P.bin_params(f, True)
     cb = L.make_bins(mode, bp, na, True)
     gamma = 10 * P.EPS32

@@ -61,12 +61,18 @@ enum { SSQB_F32 = 0, SSQB_F64 = 1, SSQB_F32X = 2 };
  * kind 1 GMW L1:   p = {gamma, beta, wc = (beta/gamma)^(1/gamma), log(wc)}
  * kind 2 GMW L2:   p = {gamma, beta, wc, sqrt(2 pi gamma 2^r / Gamma(r))}
  * band = {w_lo, w_hi}: psih is taken as 0 outside [w_lo, w_hi] (where it is
- * below ~1e-30 of its peak); band[0] >= band[1] evaluates everywhere. */
+ * below ~1e-30 of its peak); band[0] >= band[1] evaluates everywhere.
+ * npoly > 0 (GMW only; at most 8): higher-order GMW (_gmw.py:268-347). The
+ * constant factor (2 for L1, p[3] for L2) becomes the polynomial
+ * C(w) = sum_{m < npoly} kc[m] (2 w^gamma)^m, Laguerre constants times the
+ * order-k norm (_gmw.py:368-396); an average over orders (_cwt.py:517-610)
+ * is the mean of the orders' coefficient vectors. */
 typedef struct ssqb_wavelet {
   int32_t kind;
-  int32_t reserved;
+  int32_t npoly;
   double p[4];
   double band[2];
+  double kc[8];
 } ssqb_wavelet;
 
 /* Bin mapping of the squeeze (algos.py:81-87, 356-374).

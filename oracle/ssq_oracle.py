@@ -70,6 +70,11 @@ def psih(kind, params, w):
                                                      (_gmw.py:187-210, 638)
     kind 'gmw_l2': params (gamma, beta): sqrt(2pi gamma 2^r / Gamma(r))
       w^beta exp(-w^gamma), r = (2beta+1)/gamma      (_gmw.py:228-251)
+    GMW params (gamma, beta, k), k > 0: the order-k wavelet, the order-0
+      exponential times the generalized Laguerre polynomial L_k^c(2w^gamma),
+      c = r - 1, and the order-k norm: 2 sqrt(Gamma(r) k! / Gamma(k+r)) for
+      'gmw_l1', sqrt(2pi gamma 2^r k! / Gamma(k+r)) for 'gmw_l2'
+                                       (_gmw.py:268-296, 320-347, 368-396)
     """
     w = np.asarray(w, dtype=np.float64)
     if kind == 'morlet':
@@ -78,10 +83,24 @@ def psih(kind, params, w):
         ks = np.exp(-.5 * mu**2)
         C1 = np.sqrt(2) * cs * PI**.25
         return C1 * (np.exp(-.5 * (w - mu)**2) - ks * np.exp(-.5 * w**2))
-    gamma, beta = params
+    gamma, beta = params[:2]
+    k = int(params[2]) if len(params) > 2 else 0
     wc = (beta / gamma) ** (1 / gamma)
     nonneg = w >= 0
     w = w * nonneg
+    if k > 0:
+        from scipy.special import eval_genlaguerre, gammaln
+        r = (2 * beta + 1) / gamma
+        lag = eval_genlaguerre(k, r - 1, 2 * w**gamma)
+        with np.errstate(divide='ignore'):
+            if kind == 'gmw_l1':
+                norm = 2 * np.sqrt(np.exp(gammaln(r) + gammaln(k + 1) - gammaln(k + r)))
+                base = np.exp(-beta * np.log(wc) + wc**gamma + beta * np.log(w) - w**gamma)
+            else:
+                norm = np.sqrt(2 * PI * gamma * 2.**r
+                               * np.exp(gammaln(k + 1) - gammaln(k + r)))
+                base = np.exp(beta * np.log(w) - w**gamma)
+        return norm * lag * base * nonneg
     with np.errstate(divide='ignore'):
         if kind == 'gmw_l1':
             return 2 * np.exp(-beta * np.log(wc) + wc**gamma
@@ -132,6 +151,17 @@ def cwt(x, kind, params, scales, dt=1., padtype='reflect', l1_norm=True,
             dWx = dWx * s
     return np.ascontiguousarray(Wx), (None if dWx is None else
                                       np.ascontiguousarray(dWx))
+
+
+def cwt_higher_order(x, kind, params, orders, scales, dt=1., padtype='reflect',
+                     l1_norm=True, derivative=True):
+    """Mean over `orders` of the order-k transforms, each `cwt` with the
+    order-k GMW (cwt_higher_order, _cwt.py:586-599)."""
+    outs = [cwt(x, kind, tuple(params[:2]) + (k,), scales, dt, padtype, l1_norm,
+                derivative) for k in orders]
+    Wx = np.mean([o[0] for o in outs], axis=0)
+    dWx = np.mean([o[1] for o in outs], axis=0) if derivative else None
+    return Wx, dWx
 
 
 #### phase transform (algos.py:706-740, 784-816) ##############################

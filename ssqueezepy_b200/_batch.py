@@ -140,8 +140,7 @@ class SsqCwtBatch:
             ws = max(ws, xb + max(self.TUNE_BUDGETS))
         self.ws_bytes = ws
         self.ws = torch.empty(ws, dtype=torch.uint8, device=dev)
-        kind, *wp = wavelet.kernel_params()
-        self.cw = L.make_wavelet(kind, wp, wavelet.band())
+        self.cw = L.wavelet_struct(wavelet)
         self.x = torch.empty(self.n_x, dtype=torch.float32, device=dev)
         self.Wx = torch.empty(self.n_out, dtype=torch.complex64, device=dev)
         self.Tx = torch.empty(self.n_out, dtype=torch.complex64, device=dev)

@@ -21,8 +21,9 @@ PADTYPES = {'zero': 0, 'reflect': 1, 'symmetric': 2, 'replicate': 3, 'wrap': 4}
 
 
 class CWavelet(ctypes.Structure):
-    _fields_ = [('kind', ctypes.c_int32), ('reserved', ctypes.c_int32),
-                ('p', ctypes.c_double * 4), ('band', ctypes.c_double * 2)]
+    _fields_ = [('kind', ctypes.c_int32), ('npoly', ctypes.c_int32),
+                ('p', ctypes.c_double * 4), ('band', ctypes.c_double * 2),
+                ('kc', ctypes.c_double * 8)]
 
 
 class CBins(ctypes.Structure):
@@ -138,13 +139,24 @@ def ptr(t):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 
 
-def make_wavelet(kind, p, band=(0., 0.)):
+def make_wavelet(kind, p, band=(0., 0.), kc=None):
     w = CWavelet()
     w.kind = int(kind)
     for i, v in enumerate(p):
         w.p[i] = float(v)
     w.band[0], w.band[1] = float(band[0]), float(band[1])
+    if kc is not None:
+        w.npoly = len(kc)
+        for m, v in enumerate(kc[:8]):
+            w.kc[m] = float(v)
     return w
+
+
+def wavelet_struct(wavelet):
+    """The ssqb_wavelet of a `_params.Wavelet`: formula parameters, band and
+    (higher-order GMW) Laguerre coefficients."""
+    kind, *wp = wavelet.kernel_params()
+    return make_wavelet(kind, wp, wavelet.band(), wavelet.poly())
 
 
 def make_bins(mode, p, nbins, flipud):

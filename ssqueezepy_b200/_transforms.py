@@ -155,8 +155,11 @@ def _scales_plan(scales, N, wavelet, nv):
 
 #### CWT #####################################################################
 def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
-              derivative, want_idx=False, want_w=False, ssq=None, gamma=None):
-    """Run the fused CWT kernel. Returns dict of device tensors + params."""
+              derivative, want_idx=False, want_w=False, ssq=None, gamma=None,
+              kernel=None):
+    """Run the fused CWT kernel. Returns dict of device tensors + params.
+    `kernel` (default `wavelet`) is the wavelet the transform evaluates; a
+    higher-order GMW transform takes its scales from the order-0 wavelet."""
     N = x.shape[-1]
     dt, fs, _ = P.process_fs_and_t(fs, t, N)
     wavelet = P.Wavelet._init_if_not_isinstance(wavelet)
@@ -190,8 +193,7 @@ def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
     wsb = L.load().ssqb_cwt_workspace_bytes(B, N, Npad, na, prec)
     ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     sc_d = _on_device(sp, 'scales', dev)
-    kind, *wp = wavelet.kernel_params()
-    cw = L.make_wavelet(kind, wp, wavelet.band())
+    cw = L.wavelet_struct(kernel or wavelet)
     cb = L.make_bins(*ssq) if ssq is not None else None
     gamma = _default_gamma(dtype) if gamma is None else gamma
     with torch.cuda.device(dev):
@@ -216,8 +218,10 @@ def cwt(x, wavelet='gmw', scales='log-piecewise', fs=None, t=None, nv=32,
     (_cwt.py:12-320). `vectorized`, `cache_wavelet` and `patience` only
     select CPU strategies in the reference and have no effect here."""
     if isinstance(order, (tuple, list, range)) or order > 0:
-        raise NotImplementedError("higher-order GMW `cwt` (order > 0) is not on "
-                                  "the accelerated path")
+        return _cwt_higher_order(x, wavelet, order, average, astensor, dict(
+            scales=scales, fs=fs, t=t, nv=nv, l1_norm=l1_norm,
+            derivative=derivative, padtype=padtype, rpadded=rpadded,
+            nan_checks=nan_checks))
     if not isinstance(scales, str):
         nv = None
     wavelet = P.process_gmw_wavelet(wavelet, l1_norm)
@@ -246,6 +250,58 @@ def cwt(x, wavelet='gmw', scales='log-piecewise', fs=None, t=None, nv=32,
     scales_out = _scales_out(r, astensor)
     Wx, dWx = _out(Wx, astensor, r['is_2d']), _out(dWx, astensor, r['is_2d'])
     return (Wx, scales_out, dWx) if derivative else (Wx, scales_out)
+
+
+def _gmw_options(wavelet, N):
+    """The options of a GMW `wavelet` without its order, for building its
+    other orders (cwt_higher_order, _cwt.py:551-560)."""
+    base = P.Wavelet._init_if_not_isinstance(wavelet, N=N)
+    if not base.name.lower().startswith('gmw'):
+        raise ValueError("`wavelet` must be GMW for higher-order transforms "
+                         "(got %s)" % base.name)
+    opts = dict(base.config, dtype=base.dtype)
+    opts.pop('order', None)
+    return opts
+
+
+def _order0_scales(scales, N, opts, nv):
+    """String scales of a higher-order transform come from the order-0
+    wavelet (_cwt.py:573-578); an array passes through."""
+    if not isinstance(scales, str):
+        return scales
+    wav0 = P.Wavelet(('gmw', dict(opts, order=0)))
+    return _scales_plan(scales, N, wav0, nv)['scales'].reshape(-1, 1)
+
+
+def _cwt_higher_order(x, wavelet, order, average, astensor, kw):
+    """`cwt` with higher-order GMWs (cwt_higher_order, _cwt.py:517-610).
+    The transform is linear in the wavelet, so the mean over orders is one
+    transform with the mean wavelet, whose Laguerre coefficients are the
+    mean of the orders' (`Wavelet.poly`); `average=False` runs one transform
+    per order and returns lists. Scales come back as a column (na, 1), as
+    the reference returns them on this path."""
+    if isinstance(order, (list, range)):
+        order = tuple(order)
+    orders = order if isinstance(order, tuple) else (order,)
+    P._check_order(orders)
+    if len(orders) == 1 and average:
+        warnings.warn("`average` ignored with single `order`")
+        average = False
+    N = x.shape[-1]
+    opts = _gmw_options(wavelet, N)
+    scales = _order0_scales(kw.pop('scales'), N, opts, kw['nv'])
+    avg = average or (average is None and isinstance(order, tuple))
+    groups = [orders] if avg else [(k,) for k in orders]
+    outs = [cwt(x, P.Wavelet(('gmw', dict(opts, order=g))), scales=scales, order=0,
+                astensor=astensor, **kw) for g in groups]
+    derivative = kw['derivative']
+    Wx = [o[0] for o in outs]
+    dWx = [o[-1] for o in outs] if derivative else None
+    if len(outs) == 1:
+        Wx = Wx[0]
+        dWx = dWx[0] if derivative else None
+    sc = outs[0][1].reshape(-1, 1)
+    return (Wx, sc, dWx) if derivative else (Wx, sc)
 
 
 def _grad_checks(astensor, rpadded, padtype):
@@ -344,14 +400,24 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
     if x.ndim == 2 and get_w:
         raise NotImplementedError("`get_w=True` unsupported with batched input.")
     _check_ssq_args(squeezing, maprange, difftype)
-    if isinstance(order, (tuple, list, range)) or order > 0:
-        raise NotImplementedError("higher-order GMW `ssq_cwt` (order > 0) is not "
-                                  "on the accelerated path")
     if nv is None and not isinstance(scales, np.ndarray):
         nv = 32
     N = x.shape[-1]
     dt, fs, _ = P.process_fs_and_t(fs, t, N)
     wavelet = P.Wavelet._init_if_not_isinstance(wavelet, N=N)
+    kernel = None
+    if isinstance(order, (tuple, list, range)) or order > 0:
+        # higher-order GMW (_ssq_cwt.py:227-243): the transform with the mean
+        # wavelet of a tuple of orders, or with order k alone; its derivative
+        # (the reference's trigdiff of the padded transform) is the same
+        # frequency-domain derivative the fused kernel takes. The squeeze keeps
+        # the user's wavelet for `maprange`.
+        if isinstance(order, (list, range)):
+            order = tuple(order)
+        P._check_order(order)
+        opts = _gmw_options(wavelet, N)
+        scales = _order0_scales(scales, N, opts, nv)
+        kernel = P.Wavelet(('gmw', dict(opts, order=order)))
     sp = _scales_plan(scales, N, wavelet, nv)
     sc, cwt_st, na, nv_ = sp['scales'], sp['scaletype'], sp['na'], sp['nv']
 
@@ -360,7 +426,8 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
     def run(xin):
         r = _cwt_core(xin, wavelet, scales, nv, fs, t, padtype, False, nan_checks,
                       get_dWx, want_idx=True, want_w=get_w,
-                      ssq=(fp['mode'], fp['bp'], na, flipud), gamma=gamma)
+                      ssq=(fp['mode'], fp['bp'], na, flipud), gamma=gamma,
+                      kernel=kernel)
         Tx = torch.empty_like(r['Wx'])
         cst = _on_device(fp, 'const', r['dev'])
         with torch.cuda.device(r['dev']):

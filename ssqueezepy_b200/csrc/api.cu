@@ -107,6 +107,15 @@ static int check_wavelet(const ssqb_wavelet* w, WavDev* out) {
     out->ibeta = (int)w->p[1];
   if (w->kind != 0 && !(w->p[0] > 0 && w->p[1] > 0))
     return fail(SSQB_EINVAL, "GMW gamma and beta must be positive");
+  if (w->npoly < 0 || w->npoly > 8)
+    return fail(SSQB_EINVAL, "wavelet npoly must be in [0, 8]");
+  if (w->npoly > 0 && w->kind == 0)
+    return fail(SSQB_EINVAL, "wavelet npoly > 0 is for GMW kinds only");
+  out->npoly = w->npoly;
+  for (int m = 0; m < 8; ++m) {
+    out->kc[m] = m < w->npoly ? w->kc[m] : 0.0;
+    if (!std::isfinite(out->kc[m])) return fail(SSQB_EINVAL, "wavelet kc must be finite");
+  }
   return SSQB_OK;
 }
 

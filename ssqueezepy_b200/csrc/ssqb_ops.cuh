@@ -13,7 +13,19 @@ struct WavDev {
   double wcg;        // GMW: wc^gamma
   double lo, hi;     // psih = 0 outside [lo, hi] (skipped when lo >= hi)
   int ibeta;         // GMW L1: beta when it is an integer in [0, 128], else -1
+  int npoly;         // GMW order > 0: the factor 2 | l2norm becomes C(2 w^gamma)
+  double kc[8];      // C's coefficients, zero from npoly on
 };
+
+// Higher-order GMW factor C = sum_m kc[m] y^m, y = 2 x^gamma (Horner; the
+// zero coefficients past npoly leave it exact)
+__device__ __forceinline__ double gmw_poly(const WavDev& w, double xg) {
+  const double y = 2.0 * xg;
+  double c = w.kc[7];
+#pragma unroll
+  for (int m = 6; m >= 0; --m) c = fma(c, y, w.kc[m]);
+  return c;
+}
 
 // x^n for 0 <= n < 256 by binary powering (relative error ~ a few ulps)
 __device__ __forceinline__ double powi(double x, int n) {
@@ -100,18 +112,23 @@ __device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
   if (x <= 0.0) return 0.0;
   if (w.kind == 1 && w.ibeta >= 0 && w.p0 == 3.0) {
     // 2 exp(beta ln(x/wc) - (x^3 - wc^3)) = 2 (x/wc)^beta exp(wc^3 - x^3)
-    const double e = w.wcg - x * x * x;
-    return e > -708.0 ? 2.0 * powi(x / w.p2, w.ibeta) * exp(e) : 0.0;
+    const double x3 = x * x * x;
+    const double e = w.wcg - x3;
+    if (!(e > -708.0)) return 0.0;
+    const double f = w.npoly ? gmw_poly(w, x3) : 2.0;
+    return f * powi(x / w.p2, w.ibeta) * exp(e);
   }
   const double lw = log(x);
   const double xg = (w.p0 == 3.0) ? x * x * x : exp(w.p0 * lw);
   if (w.kind == 1) {
     const double e = -w.p1 * w.p3 + w.wcg + w.p1 * lw - xg;
-    return e > -708.0 ? 2.0 * exp(e) : 0.0;
+    if (!(e > -708.0)) return 0.0;
+    return (w.npoly ? gmw_poly(w, xg) : 2.0) * exp(e);
   }
   // L2: norm * x^beta * exp(-x^gamma)
   const double e = w.p1 * lw - xg;
-  return e > -708.0 ? w.p3 * exp(e) : 0.0;
+  if (!(e > -708.0)) return 0.0;
+  return (w.npoly ? gmw_poly(w, xg) : w.p3) * exp(e);
 }
 
 // ---- frequency bin (algos.py:859-953; round = half-to-even, as numba) ----

@@ -58,6 +58,9 @@ def _cwt_call(**kw):
     (dict(Wx=None), L.EINVAL),
     (dict(wsb=16), L.EWORKSPACE),
     (dict(wav=L.make_wavelet(7, (0, 0, 0, 0))), L.EINVAL),
+    (dict(wav=L.make_wavelet(0, (6., 1e-8, 1., 0.), kc=[1., 2.])), L.EINVAL),
+    (dict(wav=L.make_wavelet(1, (3., 60., 1., 0.), kc=[1.] * 9)), L.EINVAL),
+    (dict(wav=L.make_wavelet(1, (3., 60., 1., 0.), kc=[1., float('nan')])), L.EINVAL),
     (dict(idx=ctypes.c_void_p(8), bins=None), L.EINVAL),
     (dict(idx=ctypes.c_void_p(8), bins=L.make_bins(0, (0., 0.1, 0, 0, 0), 11, 1)),
      L.EINVAL),

@@ -77,3 +77,141 @@ def test_higher_order_band_covers_the_wavelet():
     v = np.abs(w.fn(grid))
     out = (grid < lo) | (grid > hi)
     assert v[out].max() <= 1e-12 * v.max() * 10
+
+
+def test_higher_order_needs_a_gmw():
+    import ssqueezepy_b200 as sb
+    x = np.zeros(64)
+    with pytest.raises(ValueError):
+        sb.cwt(x, 'morlet', order=1)
+    with pytest.raises(ValueError):
+        sb.ssq_cwt(x, 'morlet', order=(0, 1))
+
+
+def test_struct_carries_the_coefficients():
+    from ssqueezepy_b200 import _lib as L
+    w = P.Wavelet(('gmw', {'order': (0, 1, 2)}))
+    cw = L.wavelet_struct(w)
+    assert cw.npoly == 3 and np.allclose(list(cw.kc)[:3], w.poly())
+    assert list(cw.kc)[3:] == [0.] * 5
+    assert L.wavelet_struct(P.Wavelet('gmw')).npoly == 0
+    assert L.wavelet_struct(P.Wavelet('morlet')).npoly == 0
+
+
+#### GPU ######################################################################
+def _gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    return torch
+
+
+W64 = ('gmw', {'dtype': 'float64'})
+
+
+@pytest.mark.gpu
+def test_cwt_order2_matches_reference():
+    _gpu()
+    import ssqueezepy_b200 as sb
+    g = golden('higher')
+    Wx, sc = sb.cwt(g['x'], W64, order=2, astensor=False)
+    assert sc.shape == (g['scales'].shape[0], 1)
+    assert np.allclose(sc, g['scales'], rtol=1e-12, atol=0)
+    assert rel_l2(Wx, g['cwt_o2_Wx']) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_cwt_average_of_orders_matches_reference():
+    _gpu()
+    import ssqueezepy_b200 as sb
+    g = golden('higher')
+    Wx, _ = sb.cwt(g['x'], W64, order=(0, 1, 2), astensor=False)
+    assert rel_l2(Wx, g['cwt_avg012_Wx']) <= 1e-10
+    Wx, _ = sb.cwt(g['x'], W64, order=range(3), average=True, astensor=False)
+    assert rel_l2(Wx, g['cwt_avg012_Wx']) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_ssq_cwt_average_of_orders_matches_reference():
+    _gpu()
+    import ssqueezepy_b200 as sb
+    g = golden('higher')
+    Tx, Wx, f, sc = sb.ssq_cwt(g['x'], W64, order=(0, 1), astensor=False)
+    assert np.allclose(f, g['ssq_avg01_f'], rtol=1e-12, atol=0)
+    assert rel_l2(Tx, g['ssq_avg01_Tx']) <= 1e-9
+
+
+@pytest.mark.gpu
+def test_cwt_orders_unaveraged_are_the_single_orders():
+    _gpu()
+    import ssqueezepy_b200 as sb
+    g = golden('higher')
+    Ws, sc = sb.cwt(g['x'], W64, order=(1, 2), average=False, astensor=False)
+    assert isinstance(Ws, list) and len(Ws) == 2
+    assert rel_l2(Ws[1], g['cwt_o2_Wx']) <= 1e-10
+    W1, _ = sb.cwt(g['x'], ('gmw', {'dtype': 'float64', 'order': 1}),
+                   scales=sc, astensor=False)
+    assert rel_l2(Ws[0], W1) <= 1e-14
+
+
+@pytest.mark.gpu
+def test_cwt_order2_float32_within_the_float32_bar():
+    _gpu()
+    import ssqueezepy_b200 as sb
+    g = golden('higher')
+    Wx, _ = sb.cwt(g['x'].astype(np.float32), 'gmw', order=2, astensor=False)
+    assert Wx.dtype == np.complex64
+    assert rel_l2(Wx, g['cwt_o2_Wx']) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_cwt_higher_order_gradient_is_the_adjoint():
+    """The loss Re<G, Wx> is linear in x, so its gradient g satisfies
+    <g, x> = loss(x) for every x: the adjoint transform carries the
+    polynomial too."""
+    torch = _gpu()
+    import ssqueezepy_b200 as sb
+    rng = np.random.default_rng(5)
+    x = torch.tensor(rng.standard_normal(512), device='cuda', requires_grad=True)
+    Wx, _ = sb.cwt(x, W64, order=(0, 2))
+    G = torch.tensor(rng.standard_normal(tuple(Wx.shape)) +
+                     1j * rng.standard_normal(tuple(Wx.shape)), device='cuda')
+    loss = (G.conj() * Wx).real.sum()
+    loss.backward()
+    lin = float((x.grad * x.detach()).sum())
+    assert abs(lin - float(loss)) <= 1e-10 * abs(float(loss))
+
+
+def test_oracle_restates_the_reference():
+    """The oracle's order-k GMW (generalized Laguerre polynomial from scipy)
+    and its mean over orders against the reference's transforms."""
+    from oracle import ssq_oracle as O
+    g = golden('higher')
+    sc = g['scales'].ravel()
+    # scipy's Laguerre recurrence and the reference's power sum round
+    # differently where the polynomial's terms cancel: 1e-10 of the peak
+    assert np.abs(O.psih('gmw_l1', (3., 60., 1), g['psih_w']) - g['psih_o1']).max() \
+        <= 1e-10 * np.abs(g['psih_o1']).max()
+    assert np.abs(O.psih('gmw_l2', (3., 60., 3), g['psih_w']) - g['psih_o3e']).max() \
+        <= 1e-10 * np.abs(g['psih_o3e']).max()
+    Wx, _ = O.cwt(g['x'], 'gmw_l1', (3., 60., 2), sc, derivative=False)
+    assert rel_l2(Wx, g['cwt_o2_Wx']) <= 1e-12
+    Wx, _ = O.cwt_higher_order(g['x'], 'gmw_l1', (3., 60.), (0, 1, 2), sc,
+                               derivative=False)
+    assert rel_l2(Wx, g['cwt_avg012_Wx']) <= 1e-12
+
+
+def test_host_polynomial_equals_the_oracle_laguerre():
+    """Wavelet.poly (used by the kernels) against scipy's generalized
+    Laguerre polynomial in the oracle, orders 1..7, both norms. The power sum
+    in 2 w^gamma cancels more with each order (its terms grow far above
+    their sum near the peak), so the two evaluations part by about
+    8x per order: 4e-14 of the peak at k = 1, 3e-9 at k = 7."""
+    from oracle import ssq_oracle as O
+    ws = np.linspace(0, 8, 401)
+    for norm, kind in (('bandpass', 'gmw_l1'), ('energy', 'gmw_l2')):
+        for k in range(1, P.MAX_GMW_ORDER + 1):
+            w = P.Wavelet(('gmw', {'order': k, 'norm': norm, 'dtype': 'float64'}))
+            ref = O.psih(kind, (3., 60., k), ws)
+            tol = 2e-14 * 8.**k
+            assert np.abs(w.fn(ws) - ref).max() <= tol * np.abs(ref).max(), (norm, k)

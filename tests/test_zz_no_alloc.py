@@ -28,10 +28,9 @@ def _setup(N, dtype='float32'):
     Npad, n1, _ = P.p2up(N)
     dev = torch.device('cuda', 0)
     x = torch.as_tensor(chirp_signal(N, seed=3).astype(np.float32), device=dev)
-    kind, *wp = w.kernel_params()
     return dict(N=N, na=na, Npad=Npad, n1=n1, x=x, dev=dev,
                 sc=torch.as_tensor(sc.ravel(), dtype=torch.float64, device=dev),
-                cw=L.make_wavelet(kind, wp, w.band()), cb=L.make_bins(mode, bp, na, True))
+                cw=L.wavelet_struct(w), cb=L.make_bins(mode, bp, na, True))
 
 
 def _outputs(c):
