@@ -320,6 +320,39 @@ SSQB_API int ssqb_stft_adjoint(const void* gSx, const void* gTx, const uint16_t*
                                const double* window, int precision, void* gx, int accumulate,
                                void* workspace, size_t workspace_bytes, void* stream);
 
+/* Phase transform by differences along time (difftype 'phase' and
+ * 'numeric' of ssq_cwt / phase_cwt). Each of the B*na rows of Wx is ncol
+ * wide; the transform reads columns col0 .. col0+M-1 and writes w (B, na, M).
+ *   mode 1, 'phase' (_ssq_cwt.py:490-496): w[j] = |u[j+1] - u[j]| / 2pi for
+ *     j < M-1 and |u[M-1] - u[0]| / 2pi, u the angle of Wx unwrapped along
+ *     time (numpy unwrap: steps of size pi or more moved into [-pi, pi]);
+ *   mode 2, 'numeric' (phase_cwt_num, _ssq_cwt.py:512-586): w = |Im(D/Wx)| /
+ *     2pi, D the difference of order `difforder` (1 forward, 2 second-order
+ *     forward, 4 central) over dt, periodic within the M columns;
+ * w = inf where |Wx| < gamma. Arithmetic in float64 for either precision. */
+SSQB_API int ssqb_phase_diff(const void* Wx, int B, int na, int ncol, int col0, int M,
+                             int mode, int difforder, double dt, double gamma,
+                             int precision, void* w, void* stream);
+
+/* Workspace bytes of ssqb_istft: the real frames, B * n_fft * n_frames
+ * elements of the data precision. */
+SSQB_API size_t ssqb_istft_workspace_bytes(int B, int n_fft, int n_frames, int precision);
+
+/* Inverse STFT (istft, _stft.py:184-256): per frame the inverse real FFT of
+ * Sx's column (n_fft/2+1 bins; the imaginary parts of the DC and Nyquist bins
+ * are ignored), fftshifted when modulated, overlap-added at hop with
+ * wa = window^win_exp (utils/stft_utils.py:141-182), divided by the window
+ * norm sum_{t < (N-1)/hop+1} w1[p - t hop], w1 = window^(win_exp+1)
+ * (utils/stft_utils.py:169-191), where the norm exceeds `tiny` (the smallest
+ * normal number of the data type, _stft.py:245-250), and unpadded by
+ * n_fft/2 samples on the left. Sx (B, n_fft/2+1, n_frames); wa, w1 (n_fft)
+ * double; x (B, N) real. The frames must end inside the padded signal:
+ * (n_frames - 1) * hop <= N - 1. */
+SSQB_API int ssqb_istft(const void* Sx, int B, int n_fft, int n_frames, int hop, int N,
+                        int modulated, const double* wa, const double* w1, double tiny,
+                        int precision, void* x, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
 /* Gradient of Wx through the squeeze, a gather through the bin index:
  * gWx[b, i, j] = row_weights[i] * gTx[b, idx[b, i, j], j] (0 where idx is
  * 0xFFFF). Transpose of ssqb_squeeze. */

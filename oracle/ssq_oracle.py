@@ -175,6 +175,33 @@ def phase_cwt(Wx, dWx, gamma):
     return w
 
 
+def phase_unwrap(Wx, gamma):
+    """difftype='phase' (_ssq_cwt.py:490-496): steps of the angle of Wx
+    unwrapped along time, the last column u[-1] - u[0]; |.| / 2pi, inf where
+    |Wx| < gamma."""
+    u = np.unwrap(np.angle(Wx), axis=-1)
+    w = np.concatenate([np.diff(u, axis=-1), u[..., -1:] - u[..., :1]], axis=-1)
+    w = np.abs(w / (2 * PI))
+    w[np.abs(Wx) < gamma] = np.inf
+    return w
+
+
+def phase_numeric(Wx, dt, order, gamma):
+    """phase_cwt_num (_ssq_cwt.py:512-586): periodic differences of order
+    1, 2 or 4 along time, |Im(D Wx / Wx)| / 2pi, inf where |Wx| < gamma."""
+    def sh(k):  # W[j + k], periodic
+        return np.roll(Wx, -k, axis=-1)
+    if order == 1:
+        D = (sh(1) - Wx) / dt
+    elif order == 2:
+        D = (-sh(2) + 4 * sh(1) - 3 * Wx) / (2 * dt)
+    else:
+        D = (-sh(2) + 8 * sh(1) - 8 * sh(-1) + sh(-2)) / (12 * dt)
+    w = np.abs(np.imag(D / Wx) / (2 * PI))
+    w[np.abs(Wx) < gamma] = np.inf
+    return w
+
+
 def phase_stft(Sx, dSx, Sfs, gamma):
     """|Sfs_i - Im(dS conj(S)) / (|S|^2 2pi)|; inf where |S| < gamma."""
     A, B = dSx.real, dSx.imag
@@ -446,6 +473,35 @@ def stft_adjoint(gS, window, n_fft, N, hop=1, padtype='reflect', modulated=True)
 
 
 #### inverse synchrosqueezing (_ssq_cwt.py:313-400, _ssq_stft.py:139-198) ####
+def istft(Sx, window, n_fft, hop=1, N=None, modulated=True, win_exp=1):
+    """Inverse STFT of one-sided `Sx` (n_fft//2+1, n_frames) with the
+    n_fft-long `window` (_stft.py:184-256): irfft per frame, fftshift when
+    modulated, overlap-add with window^win_exp (utils/stft_utils.py:141-182),
+    divide by the window norm of window^(win_exp+1) over (N-1)//hop + 1 hops
+    (:169-191) where it exceeds the data type's tiny, unpad n_fft//2 on the
+    left. Arithmetic in the window's dtype, as the reference."""
+    nframes = Sx.shape[1]
+    N = N or hop * nframes
+    dtype = np.float32 if Sx.dtype == np.complex64 else np.float64
+    window = np.asarray(window).astype(dtype)
+    xbuf = np.fft.irfft(Sx, n=n_fft, axis=0).astype(dtype)
+    if modulated:
+        xbuf = np.fft.fftshift(xbuf, axes=0)
+    wa = np.ones_like(window) if win_exp == 0 else window ** win_exp
+    Lx = N + n_fft - 1
+    x = np.zeros(Lx, dtype=dtype)
+    for i in range(nframes):
+        x[i * hop:i * hop + n_fft] += xbuf[:, i] * wa
+    wn = np.zeros(Lx)
+    w1 = window ** (win_exp + 1)
+    for i in range((Lx - n_fft) // hop + 1):
+        wn[i * hop:i * hop + n_fft] += w1
+    th = np.finfo(dtype).tiny
+    keep = wn > th
+    x[keep] = x[keep] / wn[keep]
+    return x[n_fft // 2:Lx - (n_fft - 1) // 2]
+
+
 def issq(Tx, scale, cc=None, cw=None):
     """scale * sum_k Re Tx[k] (full inversion) or, with curve centres `cc` and
     widths `cw` (N, K), the K components summed over their row bands

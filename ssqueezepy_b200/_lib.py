@@ -69,6 +69,9 @@ SIGNATURES = {
     'ssqb_stft_adjoint_workspace_bytes': (_sz, [_i, _i, _i, _i, _i]),
     'ssqb_stft_adjoint': (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _i,
                                _vp, _i, _vp, _sz, _vp]),
+    'ssqb_phase_diff': (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _d, _d, _i, _vp, _vp]),
+    'ssqb_istft_workspace_bytes': (_sz, [_i, _i, _i, _i]),
+    'ssqb_istft': (_i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _d, _i, _vp, _vp, _sz, _vp]),
     'ssqb_squeeze_adjoint': (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _i, _vp]),
     'ssqb_icwt_adjoint': (_i, [_vp, _vp, _i, _i, _i, _i, _vp, _i, _vp]),
     'ssqb_squeeze_batch': (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),

@@ -322,7 +322,9 @@ def _scales_out(r, astensor):
     return s
 
 
-def _check_ssq_args(squeezing, maprange, difftype):
+def _check_ssq_args(squeezing, maprange, difftype, get_w=True, difforder=None):
+    """The argument checks of ssqueezing.py:314-368; returns `difforder`
+    (4 by default for difftype='numeric')."""
     if not isinstance(squeezing, str):
         raise NotImplementedError("custom `squeezing` functions are not on the "
                                   "accelerated path")
@@ -345,8 +347,17 @@ def _check_ssq_args(squeezing, maprange, difftype):
     if difftype not in ('trig', 'phase', 'numeric'):
         raise ValueError("`difftype` must be one of: direct, phase, numeric"
                          " (got %s)" % difftype)
-    if difftype != 'trig':
-        raise ValueError("GPU computation only supports `difftype = 'trig'`")
+    if difftype != 'trig' and not get_w:
+        raise ValueError("`difftype != 'trig'` requires `get_w = True`")
+    if difforder is not None:
+        if difftype != 'numeric':
+            warnings.warn("`difforder` is ignored if `difftype != 'numeric'")
+        elif difforder not in (1, 2, 4):
+            raise ValueError("`difforder` must be one of: 1, 2, 4 "
+                             "(got %s)" % difforder)
+    elif difftype == 'numeric':
+        difforder = 4
+    return difforder
 
 
 def _ssq_freqs_for_cwt(ssq_freqs, scales, N, wavelet, cwt_scaletype, maprange,
@@ -399,7 +410,7 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
     high to low (ssqueezing.py:216-224)."""
     if x.ndim == 2 and get_w:
         raise NotImplementedError("`get_w=True` unsupported with batched input.")
-    _check_ssq_args(squeezing, maprange, difftype)
+    difforder = _check_ssq_args(squeezing, maprange, difftype, get_w, difforder)
     if nv is None and not isinstance(scales, np.ndarray):
         nv = 32
     N = x.shape[-1]
@@ -421,6 +432,10 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
     sp = _scales_plan(scales, N, wavelet, nv)
     sc, cwt_st, na, nv_ = sp['scales'], sp['scaletype'], sp['na'], sp['nv']
 
+    if difftype != 'trig':
+        return _ssq_cwt_by_differences(
+            x, wavelet, kernel, scales, nv, fs, t, dt, padtype, nan_checks, gamma, sp,
+            ssq_freqs, maprange, flipud, difftype, difforder, astensor, get_dWx)
     fp = _ssq_plan(wavelet, scales, N, nv, ssq_freqs, maprange, padtype, dt, sp)
     f_asc = fp['f_asc']
     def run(xin):
@@ -454,6 +469,55 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
            _scales_out(r, astensor)]
     if get_w:
         out.append(_out(r['w'], astensor, is2))
+    if get_dWx:
+        out.append(_out(r['dWx'], astensor, is2))
+    return tuple(out)
+
+
+def _ssq_cwt_by_differences(x, wavelet, kernel, scales, nv, fs, t, dt, padtype,
+                            nan_checks, gamma, sp, ssq_freqs, maprange, flipud,
+                            difftype, difforder, astensor, get_dWx):
+    """`ssq_cwt` with difftype 'phase' or 'numeric' (get_w=True): the phase
+    transform from differences of Wx along time (`ssqb_phase_diff`), then the
+    squeeze from it (`ssqb_indexed_sum`). 'numeric' works on the padded
+    transform's columns n1-4 .. n1+N+3, its squeeze sees those N+8 columns,
+    and 4 columns are trimmed from each side of Tx, w and the padded Wx
+    afterwards, as in _ssq_cwt.py:205-220, 246-300."""
+    if A.needs_grad(x):
+        raise NotImplementedError("gradients with difftype != 'trig' are not "
+                                  "implemented")
+    numeric = difftype == 'numeric'
+    if numeric and padtype is None:
+        raise NotImplementedError("difftype='numeric' needs a padded transform "
+                                  "(`padtype` not None)")
+    N = x.shape[-1]
+    r = _cwt_core(x, wavelet, scales, nv, fs, t, padtype, numeric, nan_checks,
+                  get_dWx, gamma=gamma, kernel=kernel)
+    W, B, na, dev = r['Wx'], r['B'], r['na'], r['dev']
+    col0, M = (r['n1'] - 4, N + 8) if numeric else (0, N)
+    fp = _ssq_plan(wavelet, scales, M, nv, ssq_freqs, maprange, padtype, dt, sp)
+    prec = L.F64 if r['dtype'] == 'float64' else L.F32
+    w = torch.empty((B, na, M), dtype=_RDT[r['dtype']], device=dev)
+    lib = L.load()
+    with torch.cuda.device(dev):
+        rc = lib.ssqb_phase_diff(L.ptr(W), B, na, W.shape[-1], col0, M,
+                                 2 if numeric else 1, int(difforder or 4), float(dt),
+                                 float(r['gamma']), prec, L.ptr(w), L.stream_ptr())
+        L.check(rc, 'phase_diff')
+        Ws = W[..., col0:col0 + M].contiguous() if numeric else W
+        Tx = torch.empty_like(Ws)
+        cst = _on_device(fp, 'const', dev)
+        cb = L.make_bins(fp['mode'], fp['bp'], na, flipud)
+        rc = lib.ssqb_indexed_sum(L.ptr(Ws), L.ptr(w), L.ptr(cst), cb, B, na, M, prec,
+                                  L.ptr(Tx), L.stream_ptr())
+    L.check(rc, 'squeeze')
+    if numeric:
+        # Tx and w lose the 4 extra columns each side; the returned Wx is the
+        # padded transform less 4 columns each side (_ssq_cwt.py:294-296)
+        Ws, Tx, w = (a[..., 4:-4].contiguous() for a in (W, Tx, w))
+    is2 = r['is_2d']
+    out = [_out(Tx, astensor, is2), _out(Ws, astensor, is2), fp['f_asc'][::-1],
+           _scales_out(r, astensor), _out(w, astensor, is2)]
     if get_dWx:
         out.append(_out(r['dWx'], astensor, is2))
     return tuple(out)
@@ -691,14 +755,51 @@ def ssqueeze(Wx, w=None, ssq_freqs=None, scales=None, Sfs=None, fs=None, t=None,
 
 
 def phase_cwt(Wx, dWx, difftype='trig', gamma=None):
-    """|Im(dWx / Wx)| / 2pi, inf where |Wx| < gamma (_ssq_cwt.py:420-509)."""
-    if difftype != 'trig':
-        raise ValueError("GPU computation only supports `difftype = 'trig'`")
+    """Phase transform of a CWT, inf where |Wx| < gamma (default sqrt(eps)
+    of the data type), _ssq_cwt.py:420-509: |Im(dWx / Wx)| / 2pi for
+    difftype 'trig'; for 'phase' the steps of the angle of Wx unwrapped along
+    time (`dWx` unused), the last column the whole unwrapped excursion."""
+    if difftype not in ('trig', 'phase'):
+        raise ValueError(f"unsupported `difftype` '{difftype}'; must be one of "
+                         "'trig', 'phase'.")
     W = torch.as_tensor(Wx)
+    if gamma is None:
+        gamma = np.sqrt(P.EPS64 if W.dtype == torch.complex128 else P.EPS32)
+    if difftype == 'phase':
+        return _phase_diff(W, 1, 4, 1., gamma)
     dW = torch.as_tensor(dWx)
-    gamma = _default_gamma('float64' if W.dtype == torch.complex128 else
-                           'float32') if gamma is None else gamma
     return _phase(W, dW, None, gamma)
+
+
+def phase_cwt_num(Wx, dt, difforder=4, gamma=None):
+    """Phase transform from numeric differences of Wx along time, periodic
+    over the row (phase_cwt_num, _ssq_cwt.py:512-586): |Im(D Wx / Wx)| / 2pi,
+    D of order 1, 2 or 4; inf where |Wx| < gamma (default 10 eps)."""
+    if difforder not in (1, 2, 4):
+        raise ValueError("`difforder` must be one of: 1, 2, 4 "
+                         "(got %s)" % difforder)
+    W = torch.as_tensor(Wx)
+    gamma = gamma or _default_gamma('float64' if W.dtype == torch.complex128 else
+                                    'float32')
+    return _phase_diff(W, 2, difforder, dt, gamma)
+
+
+def _phase_diff(W, mode, difforder, dt, gamma):
+    if not W.is_complex():
+        raise ValueError("`Wx` must be complex")
+    L.require_cuda()
+    dev = _device_of(W)
+    W3 = W.to(dev).contiguous()
+    W3 = W3 if W3.ndim == 3 else W3[None]
+    B, na, N = W3.shape
+    prec = L.F64 if W3.dtype == torch.complex128 else L.F32
+    w = torch.empty((B, na, N), dtype=W3.real.dtype, device=dev)
+    with torch.cuda.device(dev):
+        rc = L.load().ssqb_phase_diff(L.ptr(W3), B, na, N, 0, N, mode, int(difforder),
+                                      float(dt), float(gamma), prec, L.ptr(w),
+                                      L.stream_ptr())
+    L.check(rc, 'phase_diff')
+    return w if W.ndim == 3 else w[0]
 
 
 def phase_stft(Sx, dSx, Sfs, gamma=None):
@@ -803,6 +904,84 @@ def stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=None,
         S, dS = r['Sx'], r['dSx']
     Sx, dSx = _out(S, True, r['is_2d']), _out(dS, True, r['is_2d'])
     return (Sx, dSx) if derivative else Sx
+
+
+def _istft_plan(window, win_len, n_fft, hop_len, win_exp, dtype):
+    """Window powers of the inverse STFT and the NOLA checks' warnings
+    (_stft.py:230-237, 313-337), cached. The window is rounded to the data
+    type first and its powers taken there, as the reference does."""
+    def make():
+        from scipy import signal as sig
+        win, _ = P.get_window(window, win_len, n_fft)
+        win = win.astype(dtype)
+        msgs = []
+        if hop_len > len(win):
+            msgs.append("`hop_len > len(window)`; STFT not invertible")
+        elif not sig.check_NOLA(win, len(win), len(win) - hop_len):
+            msgs.append("`window` fails Non-zero Overlap Add (NOLA) criterion; "
+                        "STFT not invertible")
+        if dtype == 'float32' and not sig.check_NOLA(win, len(win), len(win) - hop_len,
+                                                     tol=1e-3):
+            msgs.append("Imprecision expected at right-most hop of signal, in "
+                        "inversion. Lower `hop_len`, choose wider `window`, or use "
+                        "`dtype='float64'`.")
+        wa = np.ones_like(win) if win_exp == 0 else (win if win_exp == 1 else
+                                                      win ** win_exp)
+        w1 = win ** (win_exp + 1)
+        return dict(wa=np.asarray(wa, np.float64), w1=np.asarray(w1, np.float64),
+                    msgs=msgs)
+    return _plan(('istft', _akey(window), win_len, n_fft, hop_len, win_exp, dtype), make)
+
+
+def istft(Sx, window=None, n_fft=None, win_len=None, hop_len=1, N=None,
+          modulated=True, win_exp=1):
+    """Inverse STFT (_stft.py:184-256): per frame an inverse real FFT
+    (fftshifted when `modulated`), overlap-added with window^win_exp and
+    divided by the window norm sum of window^(win_exp+1), on the GPU. `Sx`
+    (n_fft//2+1, n_frames), or batched (B, n_fft//2+1, n_frames); returns
+    (N,) or (B, N), a numpy array for a numpy `Sx`, else a CUDA tensor."""
+    is_np = isinstance(Sx, np.ndarray)
+    S = torch.as_tensor(Sx)
+    if not S.is_complex():
+        raise ValueError("`Sx` must be complex")
+    is3 = S.ndim == 3
+    S3 = S if is3 else S[None]
+    if S3.ndim != 3:
+        raise ValueError("`Sx` must be 2D or 3D (got %s dims)" % S.ndim)
+    B, nrow, nframes = S3.shape
+    n_fft = n_fft or (nrow - 1) * 2
+    win_len = win_len or n_fft
+    N = N or hop_len * nframes
+    dtype = 'float32' if S.dtype == torch.complex64 else 'float64'
+    if n_fft & (n_fft - 1) or n_fft < 8 or n_fft > 4096:
+        raise NotImplementedError("n_fft must be a power of two in [8, 4096] on "
+                                  "the accelerated path (got %s)" % n_fft)
+    if nrow != n_fft // 2 + 1:
+        raise NotImplementedError("`Sx` must have n_fft//2 + 1 rows on the "
+                                  "accelerated path (got %s for n_fft=%s)" % (nrow, n_fft))
+    if (nframes - 1) * hop_len > N - 1:
+        raise ValueError("%s frames at hop_len=%s end past a signal of N=%s"
+                         % (nframes, hop_len, N))
+    ip = _istft_plan(window, win_len, n_fft, hop_len, win_exp, dtype)
+    for m in ip['msgs']:
+        warnings.warn(m)
+    L.require_cuda()
+    dev = _device_of(Sx)
+    S3 = S3.to(dev).contiguous()
+    wa, w1 = _on_device(ip, 'wa', dev), _on_device(ip, 'w1', dev)
+    prec = _prec(dtype)
+    x = torch.empty((B, N), dtype=_RDT[dtype], device=dev)
+    lib = L.load()
+    wsb = lib.ssqb_istft_workspace_bytes(B, n_fft, nframes, prec)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    with torch.cuda.device(dev):
+        rc = lib.ssqb_istft(L.ptr(S3), B, n_fft, nframes, hop_len, N,
+                            1 if modulated else 0, L.ptr(wa), L.ptr(w1),
+                            float(np.finfo(dtype).tiny), prec, L.ptr(x), L.ptr(ws), wsb,
+                            L.stream_ptr())
+    L.check(rc, 'istft')
+    x = x if is3 else x[0]
+    return x.cpu().numpy() if is_np else x
 
 
 def ssq_stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=None,

@@ -784,6 +784,76 @@ int ssqb_stft_adjoint(const void* gSx, const void* gTx, const uint16_t* idx, int
   return SSQB_OK;
 }
 
+int ssqb_phase_diff(const void* Wx, int B, int na, int ncol, int col0, int M, int mode,
+                    int difforder, double dt, double gamma, int precision, void* w,
+                    void* stream) {
+  if (!Wx || !w) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || na < 1 || M < 2) return fail(SSQB_EINVAL, "B, na must be >= 1 and M >= 2");
+  if (col0 < 0 || ncol < 1 || (long long)col0 + M > ncol)
+    return fail(SSQB_EINVAL, "columns col0 .. col0+M-1 must lie in the row");
+  if (mode != 1 && mode != 2) return fail(SSQB_EINVAL, "mode must be 1 (phase) or 2 (numeric)");
+  if (mode == 2 && difforder != 1 && difforder != 2 && difforder != 4)
+    return fail(SSQB_EINVAL, "difforder must be 1, 2 or 4");
+  if (mode == 2 && !(dt > 0)) return fail(SSQB_EINVAL, "dt must be > 0");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  const long long rows = (long long)B * na;
+  if (rows > 0x7fffffffLL) return fail(SSQB_EINVAL, "too many rows");
+  cudaStream_t st = (cudaStream_t)stream;
+  int e;
+  if (data_prec(precision) == SSQB_F64)
+    e = run_phase_diff_f64((const double2*)Wx, rows, ncol, col0, M, mode, difforder, dt, gamma,
+                           (double*)w, st);
+  else
+    e = run_phase_diff_f32((const float2*)Wx, rows, ncol, col0, M, mode, difforder, dt, gamma,
+                           (float*)w, st);
+  if (e) return cuda_fail((cudaError_t)e, "phase_diff launch");
+  return SSQB_OK;
+}
+
+size_t ssqb_istft_workspace_bytes(int B, int n_fft, int n_frames, int precision) {
+  if (B < 1 || n_frames < 1 || !is_pow2(n_fft) || !valid_precision(precision)) return 0;
+  const size_t rs = data_prec(precision) == SSQB_F64 ? sizeof(double) : sizeof(float);
+  return (size_t)B * n_fft * (size_t)n_frames * rs;
+}
+
+int ssqb_istft(const void* Sx, int B, int n_fft, int n_frames, int hop, int N, int modulated,
+               const double* wa, const double* w1, double tiny, int precision, void* x,
+               void* workspace, size_t workspace_bytes, void* stream) {
+  if (!Sx || !wa || !w1 || !x || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (B < 1 || N < 1 || hop < 1 || n_frames < 1)
+    return fail(SSQB_EINVAL, "B, N, hop and n_frames must be >= 1");
+  if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  if (!is_pow2(n_fft) || n_fft < 8 || n_fft > 4096)
+    return fail(SSQB_EUNSUPPORTED, "n_fft must be a power of two in [8, 4096]");
+  const bool f64 = data_prec(precision) == SSQB_F64;
+  if (f64 && n_fft > FftCfg<double2>::TILE)
+    return fail(SSQB_EUNSUPPORTED, "n_fft above " + std::to_string(FftCfg<double2>::TILE) +
+                                       " needs float32 data");
+  if ((long long)(n_frames - 1) * hop > (long long)N - 1)
+    return fail(SSQB_EINVAL, "frames end past the signal: need (n_frames - 1) * hop <= N - 1");
+  if (!(tiny >= 0)) return fail(SSQB_EINVAL, "tiny must be >= 0");
+  const size_t need = ssqb_istft_workspace_bytes(B, n_fft, n_frames, precision);
+  if (workspace_bytes < need)
+    return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                     " bytes");
+  Tables tb;
+  int r = get_tables(&tb);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  int e;
+  if (f64)
+    e = run_istft_f64((const double2*)Sx, B, N, n_fft, hop, n_frames, modulated ? 1 : 0, wa,
+                      w1, tiny, (double*)x, workspace, tb, st);
+  else
+    e = run_istft_f32((const float2*)Sx, B, N, n_fft, hop, n_frames, modulated ? 1 : 0, wa,
+                      w1, tiny, (float*)x, workspace, tb, st);
+  if (e) return cuda_fail((cudaError_t)e, "istft launch");
+  return SSQB_OK;
+}
+
 static int wx_adjoint(const void* gTx, const uint16_t* idx, int idx_pitch,
                       const double* sq_weights, int nbins, const void* gxr,
                       const double* icwt_weights, int B, int na, int N, int precision,

@@ -139,10 +139,15 @@ struct StftAdjOp {
   int L, nrow, nframes;
   T* gu;                                // (B, L, nframes), element-major
   int* status;
+  int interior2;                        // 1: bins 0 < f < L/2 doubled (inverse rfft)
   __device__ StftAdjOp bind(int) const { return *this; }
   __device__ int rows() const { return nframes; }
   __device__ void load(int b, int t, int f, C (&v)[1]) const {
     v[0] = f < nrow ? src.at(b, nrow, nframes, f, t, status) : mk((T)0, (T)0);
+    if (interior2 && f > 0 && f < L / 2) {
+      v[0].x *= (T)2;
+      v[0].y *= (T)2;
+    }
   }
   template <class LY>
   __device__ void store_smem(int b, int t, int n, C* const (&buf)[1], int fr) const {
@@ -174,6 +179,77 @@ __global__ void stft_adj_gather_kernel(const T* __restrict__ gu, const double* _
     }
   });
   gx[i] = accumulate ? gx[i] + acc : acc;
+}
+
+// ---- inverse STFT (_stft.py:184-256, utils/stft_utils.py:141-191) ------------
+// Frame t of the inverse is xbuf[m, t] = irfft(Sx[:, t])[m]
+//   = (1/L) Re sum_{f <= L/2} c_f Sx[f, t] e^{+2 pi i f m / L},
+// c_0 = c_{L/2} = 1, c_f = 2 otherwise (the imaginary parts of the DC and
+// Nyquist bins drop out of the real part): StftAdjOp with the interior bins
+// doubled, 1/L applied here (a power of two, so exact). A modulated frame is
+// fftshifted, for even L a rotation by L/2. Overlap-add with wa = window^a
+// over frames in ascending order, as the reference does, then divide by the
+// window norm wn[p] = sum_{t < maxhops} w1[p - t hop], w1 = window^(a+1),
+// where wn > tiny (the reference divides everywhere when min(wn) >= tiny and
+// only where wn > tiny otherwise; the two differ only where wn == tiny).
+// Output: the padded positions p = L/2 .. L/2 + N - 1 the reference keeps.
+// Sums run in double for either data precision.
+template <typename T>
+__global__ void istft_ola_kernel(const T* __restrict__ gu, const double* __restrict__ wa,
+                                 const double* __restrict__ w1, int B, int N, int L, int hop,
+                                 int nframes, int maxhops, int modulated, double tiny,
+                                 T* __restrict__ x) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)B * N) return;
+  const int b = (int)(i / N), s = (int)(i % N);
+  const T* g = gu + (size_t)b * L * nframes;
+  const int half = L / 2;
+  const long long p = (long long)s + half;
+  const long long num = p - L + 1;
+  const long long tlo = num <= 0 ? 0 : (num + hop - 1) / hop;
+  const long long tmax = p / hop;
+  const long long thi = tmax < nframes - 1 ? tmax : nframes - 1;
+  const long long tw = tmax < maxhops - 1 ? tmax : maxhops - 1;
+  double acc = 0.0, wn = 0.0;
+  for (long long t = tlo; t <= thi; ++t) {
+    const int q = (int)(p - t * hop);
+    const int m = modulated ? ((q + half) & (L - 1)) : q;
+    acc += (double)g[(size_t)m * nframes + t] * wa[q];
+  }
+  for (long long t = tlo; t <= tw; ++t) wn += w1[(int)(p - t * hop)];
+  acc *= 1.0 / L;
+  x[i] = (T)(wn > tiny ? acc / wn : acc);
+}
+
+template <typename C>
+static int run_istft(const C* Sx, int B, int N, int L, int hop, int nframes, int modulated,
+                     const double* wa, const double* w1, double tiny,
+                     typename RealOf<C>::type* x, void* ws, const Tables& tb,
+                     cudaStream_t st) {
+  typedef typename RealOf<C>::type T;
+  const int nrow = L / 2 + 1;
+  AdjSources<C> src{Sx, nullptr, nullptr, 0, nrow, nullptr, nullptr, nullptr};
+  StftAdjOp<C> op{src, L, nrow, nframes, (T*)ws, tb.status, 1};
+  int e = run_single<StftAdjOp<C>, C, 1>(op, B, nframes, ilog2(L), tb, st);
+  if (e) return e;
+  if (int* c = launch_counter()) return ++*c, 0;
+  const int maxhops = (N - 1) / hop + 1;
+  const size_t n = (size_t)B * N;
+  istft_ola_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+      (const T*)ws, wa, w1, B, N, L, hop, nframes, maxhops, modulated, tiny, x);
+  return cudaGetLastError();
+}
+
+int run_istft_f32(const float2* Sx, int B, int N, int L, int hop, int nframes, int modulated,
+                  const double* wa, const double* w1, double tiny, float* x, void* ws,
+                  const Tables& tb, cudaStream_t st) {
+  return run_istft<float2>(Sx, B, N, L, hop, nframes, modulated, wa, w1, tiny, x, ws, tb, st);
+}
+
+int run_istft_f64(const double2* Sx, int B, int N, int L, int hop, int nframes, int modulated,
+                  const double* wa, const double* w1, double tiny, double* x, void* ws,
+                  const Tables& tb, cudaStream_t st) {
+  return run_istft<double2>(Sx, B, N, L, hop, nframes, modulated, wa, w1, tiny, x, ws, tb, st);
 }
 
 template <typename C>
@@ -259,7 +335,7 @@ static int run_stft_adj(const AdjSources<C>& src, int B, int N, int L, int hop, 
                         const Tables& tb, cudaStream_t st) {
   typedef typename RealOf<C>::type T;
   const int nframes = (N - 1) / hop + 1;
-  StftAdjOp<C> op{src, L, L / 2 + 1, nframes, (T*)ws, tb.status};
+  StftAdjOp<C> op{src, L, L / 2 + 1, nframes, (T*)ws, tb.status, 0};
   int e = run_single<StftAdjOp<C>, C, 1>(op, B, nframes, ilog2(L), tb, st);
   if (e) return e;
   if (int* c = launch_counter()) return ++*c, 0;

@@ -134,6 +134,16 @@ int run_stft_adjoint_f32(const AdjSources<float2>& src, int B, int N, int L, int
 int run_stft_adjoint_f64(const AdjSources<double2>& src, int B, int N, int L, int hop, int n1,
                          int padtype, int modulated, const double* win, double* gx,
                          int accumulate, void* ws, const Tables& tb, cudaStream_t st);
+int run_istft_f32(const float2* Sx, int B, int N, int L, int hop, int nframes, int modulated,
+                  const double* wa, const double* w1, double tiny, float* x, void* ws,
+                  const Tables& tb, cudaStream_t st);
+int run_istft_f64(const double2* Sx, int B, int N, int L, int hop, int nframes, int modulated,
+                  const double* wa, const double* w1, double tiny, double* x, void* ws,
+                  const Tables& tb, cudaStream_t st);
+int run_phase_diff_f32(const float2* Wx, long long rows, int ncol, int col0, int M, int mode,
+                       int order, double dt, double gamma, float* w, cudaStream_t st);
+int run_phase_diff_f64(const double2* Wx, long long rows, int ncol, int col0, int M, int mode,
+                       int order, double dt, double gamma, double* w, cudaStream_t st);
 int run_wx_adjoint_f32(const AdjSources<float2>& src, int B, int na, int N, float2* gWx,
                        int accumulate, int* status, cudaStream_t st);
 int run_wx_adjoint_f64(const AdjSources<double2>& src, int B, int na, int N, double2* gWx,

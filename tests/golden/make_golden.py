@@ -26,7 +26,16 @@ Writes:
                    order=2, cwt averaged over orders (0, 1, 2), ssq_cwt with
                    order=(0, 1), and order-1 / order-3 wavelet samples
 
-`--only issq` / `--only ridges` / `--only higher` writes that file alone.
+  istft.npz        istft of stft outputs and of seeded complex one-sided
+                   spectra: hop, win_len < n_fft, win_exp 0 / 1 / 2,
+                   modulated on and off, float64 and float32, with inputs
+
+  difftype.npz     ssq_cwt with difftype 'phase' and 'numeric' (difforder
+                   1, 2, 4), get_w=True, float64, and phase_cwt /
+                   phase_cwt_num of the same Wx
+
+`--only issq` / `--only ridges` / `--only higher` / `--only istft` /
+`--only difftype` writes that file alone.
 """
 import os
 import sys
@@ -273,6 +282,70 @@ def higher_fixtures(ref_root):
     np.savez_compressed(os.path.join(HERE, 'higher.npz'), **out)
 
 
+ISTFT_CASES = [
+    # name, N (signal; None: the spectrum is seeded noise), n_fft, win_len,
+    # hop, window, N passed to istft, modulated, win_exp, dtype
+    ('a', 300, 64, 64, 1, 'hann', 300, True, 1, 'float64'),
+    ('b', 301, 64, 48, 4, 'hann', 301, True, 0, 'float64'),
+    ('c', None, 64, 64, 3, 'hann', None, False, 1, 'float64'),
+    ('d', None, 32, 32, 2, None, None, True, 2, 'float64'),
+    ('e', 300, 64, 64, 1, 'hann', 300, True, 1, 'float32'),
+    ('f', 600, 512, 512, 4, 'hann', 600, True, 1, 'float64'),
+    ('g', 1000, 128, 100, 5, 'hamming', 997, False, 1, 'float64'),
+]
+
+
+def istft_fixtures(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    out = {}
+    for name, N, n_fft, win_len, hop, win, Ni, mod, wexp, dt in ISTFT_CASES:
+        if N is not None:
+            x = chirp_signal(N, seed=len(name) + N)
+            Sx = sq.stft(x, window=win, n_fft=n_fft, win_len=win_len, hop_len=hop,
+                         modulated=mod, dtype='float64')
+            Sx = np.asarray(Sx)
+        else:
+            rng = np.random.default_rng(n_fft + hop)
+            shape = (n_fft // 2 + 1, 80)
+            Sx = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        if dt == 'float32':
+            Sx = Sx.astype(np.complex64)
+        xr = sq.istft(Sx, window=win, n_fft=n_fft, win_len=win_len, hop_len=hop,
+                      N=Ni, modulated=mod, win_exp=wexp)
+        out[name + '/Sx'] = Sx
+        out[name + '/x'] = np.asarray(xr)
+    np.savez_compressed(os.path.join(HERE, 'istft.npz'), **out)
+
+
+def difftype_fixtures(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    from ssqueezepy import Wavelet
+    from ssqueezepy._ssq_cwt import phase_cwt, phase_cwt_num
+    x = chirp_signal(256, seed=6)
+    out = dict(x=x)
+    w = Wavelet(('gmw', dict(dtype='float64')))
+    Tx, Wx, f, sc, wp = sq.ssq_cwt(x, w, nv=8, difftype='phase', get_w=True,
+                                   astensor=False)
+    out.update({'phase/Tx': Tx, 'phase/f': f, 'phase/w': wp})
+    for k in (1, 2, 4):
+        Tx, Wx, f, sc, wn = sq.ssq_cwt(x, w, nv=8, difftype='numeric', difforder=k,
+                                       get_w=True, astensor=False)
+        out.update({'num%d/Tx' % k: Tx, 'num%d/w' % k: wn, 'num%d/f' % k: f})
+    # the returned Wx of difftype='numeric' is the padded transform less 4
+    # columns on each side (_ssq_cwt.py:294-296)
+    out['num4/Wx_shape'] = np.array(Wx.shape)
+    out['num4/Wx_row0'] = Wx[0]
+    W0, _ = sq.cwt(x, w, nv=8, astensor=False)
+    out['cwt/Wx'] = W0
+    out['phase_cwt/w'] = phase_cwt(W0, None, difftype='phase')
+    out['phase_cwt_num/w'] = phase_cwt_num(W0, 1., difforder=4)
+    np.savez_compressed(os.path.join(HERE, 'difftype.npz'), **out)
+
+
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
     root = args[0] if args else '/root/reference'
@@ -282,8 +355,14 @@ if __name__ == '__main__':
         ridges_fixtures(root)
     elif '--only' in sys.argv and 'higher' in sys.argv:
         higher_fixtures(root)
+    elif '--only' in sys.argv and 'istft' in sys.argv:
+        istft_fixtures(root)
+    elif '--only' in sys.argv and 'difftype' in sys.argv:
+        difftype_fixtures(root)
     else:
         main(root)
         issq_fixtures(root)
         ridges_fixtures(root)
         higher_fixtures(root)
+        istft_fixtures(root)
+        difftype_fixtures(root)
