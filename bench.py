@@ -273,11 +273,15 @@ def run_ours(args):
     if not args.no_train:
         torch.cuda.empty_cache()
         train = run_train(args, torch, dev, world, barrier, flush)
+    next_ = None
+    if not args.no_next:
+        torch.cuda.empty_cache()
+        next_ = run_next(args, torch, dev, world, barrier, flush)
     clocks = clk.stop() if clk else None
     if rank == 0:
         emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
              launches, clocks, sc, f, const, Tx_keep, Wx_keep, batched, train, long_,
-             stft_)
+             stft_, next_)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -475,6 +479,78 @@ def run_stft(args, torch, dev, world, barrier, flush):
                          "bytes": "N (4 + 16 * 257): read x, write Sx and Tx"}}
 
 
+def run_next(args, torch, dev, world, barrier, flush):
+    """The rows beside the path, on the headline signal (N = 160,000, GMW(3,60),
+    293 rows, float32 data) through the public API with inputs resident on the
+    device: ssq_cwt with higher-order GMWs averaged over orders (0, 1), the
+    phase transform by unwrapped angle (difftype='phase', get_w=True), the
+    full inverse issq_cwt of Tx, extract_ridges of Tx (one ridge, bw 15), and
+    istft of the Hann-512 hop-1 STFT (257 x N). Each entry: mean device time
+    of `steps` calls after warm-up, L2 flushed between calls."""
+    import ssqueezepy_b200 as sb
+    rank = int(os.environ.get('RANK', 0))
+    N = args.n
+    x = torch.as_tensor(chirp_signal(N, seed=rank).astype(np.float32), device=dev)
+    st = torch.cuda.current_stream()
+    wav = ('gmw', {'gamma': 3., 'beta': 60.})
+    Tx, Wx, f, sc = sb.ssq_cwt(x, wav)
+    na = int(Tx.shape[0])
+    del Wx
+    Sx = sb.stft(x, 'hann', n_fft=512)
+
+    def timed(fn, steps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        for e in evs:
+            flush.zero_()
+            e[0].record(st)
+            fn()
+            e[1].record(st)
+        barrier()
+        return float(np.mean([a.elapsed_time(b) for a, b in evs]))
+
+    ridge_steps = max(1, min(args.steps, 3))
+    ms = [timed(lambda: sb.ssq_cwt(x, wav), args.steps),
+          timed(lambda: sb.ssq_cwt(x, wav, order=(0, 1)), args.steps),
+          timed(lambda: sb.ssq_cwt(x, wav, difftype='phase', get_w=True), args.steps),
+          timed(lambda: sb.issq_cwt(Tx, wav), args.steps),
+          timed(lambda: sb.extract_ridges(Tx, sc, penalty=2., n_ridges=1, bw=15),
+                ridge_steps),
+          timed(lambda: sb.istft(Sx, 'hann', n_fft=512, N=N), args.steps)]
+    ms = max_over_ranks(ms, dev)
+    hbm, src = peaks()
+
+    def entry(name, t, nbytes, what):
+        gbs = nbytes / (t * 1e-3) / 1e9
+        return {"workload": name, "ms": t, "value": world * N / (t * 1e-3), "unit": UNIT,
+                "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                             "frac": gbs / hbm, "bytes": what}}
+    ssq_bytes = (4 + 16 * na) * N
+    return {
+        "ssq_cwt_api": entry("ssq_cwt through the public API (reference point)", ms[0],
+                             ssq_bytes, "N (4 + 16 na): read x, write Wx and Tx"),
+        "higher_order_avg01": entry("ssq_cwt order=(0, 1): one transform with the mean "
+                                    "wavelet", ms[1], ssq_bytes,
+                                    "N (4 + 16 na): read x, write Wx and Tx"),
+        "difftype_phase": entry("ssq_cwt difftype='phase', get_w=True", ms[2],
+                                (4 + 16 * na + 16 * na + 4 * na) * N,
+                                "N (4 + 8 na + 16 na + 4 na + 8 na): x; Wx written and "
+                                "read; w; Tx"),
+        "issq_cwt": entry("issq_cwt of Tx (full inversion)", ms[3], (8 * na + 8) * N,
+                          "N (8 na + 8): read Tx, write x (float64)"),
+        "extract_ridges": dict(entry("extract_ridges of Tx, 1 ridge, bw 15", ms[4],
+                                     (8 * na + 8) * N, "N (8 na + 8): read Tx, write the "
+                                     "ridge"), note="forward sweep is sequential in "
+                                     "time: latency-bound, not HBM-bound"),
+        "istft": entry("istft of stft(x, hann, n_fft=512, hop 1) (257 x N)", ms[5],
+                       (8 * 257 + 4) * N, "N (8 * 257 + 4): read Sx, write x"),
+        "peak_source": src,
+    }
+
+
 def run_long(args, torch, dev, world, barrier):
     """Long signals: 8 float32 chirp mixtures of N = 1,048,576 (Npad 2,097,152),
     GMW(3,60), scales='log:maximal' (613 rows). Plain forward (one signal per
@@ -561,7 +637,7 @@ def run_long(args, torch, dev, world, barrier):
 
 def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
          launches, clocks, sc, f, const, Tg, Wg, batched=None, train=None, long_=None,
-         stft_=None):
+         stft_=None, next_=None):
     hbm, src = peaks()
     if True:
         alg_cwt = (4 + 8 * na) * N          # read x, write Wx
@@ -607,6 +683,8 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
             line["long"] = long_
         if stft_ is not None:
             line["stft"] = stft_
+        if next_ is not None:
+            line["next_rows"] = next_
         if world == 1 and not args.no_cpu:
             t0 = time.perf_counter()
             To, Wo, _ = oracle_step(chirp_signal(N, seed=0), sc, f, const)
@@ -643,6 +721,9 @@ def main():
                     help='skip the 8 x 1,048,576 long-signal leg')
     ap.add_argument('--no-train', action='store_true',
                     help='skip the forward + backward (training loss) leg')
+    ap.add_argument('--no-next', action='store_true',
+                    help='skip the legs of the rows beside the path (higher-order '
+                         'GMW, difftype phase, issq, ridges, istft)')
     ap.add_argument('--train-batch', type=int, default=64,
                     help='signals of N=16384 in the forward + backward leg')
     ap.add_argument('--n', type=int, default=N_SIG,

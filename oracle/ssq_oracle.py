@@ -530,6 +530,24 @@ def issq(Tx, scale, cc=None, cw=None):
 
 
 #### ridge extraction (ridge_extraction.py:11-232, serial code path) ##########
+def ridge_track(E, P, eps):
+    """Forward min-plus sweep of E (nf, N) with jump penalties P (nf, nf),
+    then the backward re-tracking: the last row whose accumulated value
+    reproduces within eps, else the column's argmin (ridge_extraction.py:
+    147-162, 187-232), in E's arithmetic type."""
+    N = E.shape[1]
+    pen = E.copy()
+    for t in range(1, N):
+        pen[:, t] += np.amin(pen[:, t - 1][None, :] + P, axis=1)
+    r = np.argmin(pen, axis=0)
+    for t in range(N - 2, -1, -1):
+        val = pen[r[t + 1], t + 1] - E[r[t + 1], t + 1]
+        hit = np.nonzero(np.abs(val - (pen[:, t] + P[r[t + 1], :])) < eps)[0]
+        if len(hit):
+            r[t] = hit[-1]
+    return r
+
+
 def extract_ridges(Tf, scales, penalty=2., n_ridges=1, bw=15, transform='cwt'):
     """(ridge_idxs, ridge_f, ridge_e), each (N, n_ridges): forward-backward
     tracking of min accumulated -log normalised energy plus
@@ -549,15 +567,7 @@ def extract_ridges(Tf, scales, penalty=2., n_ridges=1, bw=15, transform='cwt'):
     re = np.zeros((N, n_ridges), dt)
     for i in range(n_ridges):
         E = -np.log(energy / energy.max(axis=0) + eps)
-        pen = E.copy()
-        for t in range(1, N):
-            pen[:, t] += np.amin(pen[:, t - 1][None, :] + P, axis=1)
-        r = np.argmin(pen, axis=0)
-        for t in range(N - 2, -1, -1):
-            val = pen[r[t + 1], t + 1] - E[r[t + 1], t + 1]
-            hit = np.nonzero(np.abs(val - (pen[:, t] + P[r[t + 1], :])) < eps)[0]
-            if len(hit):
-                r[t] = hit[-1]
+        r = ridge_track(E, P, eps)
         idxs[:, i] = r
         rf[:, i] = scales[r]
         re[:, i] = energy[r, np.arange(N)]

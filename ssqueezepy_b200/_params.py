@@ -218,10 +218,12 @@ class Wavelet():
     @N.setter
     def N(self, value):
         self._N = value
-        self._xi = xifn(1., value)
+        self._xi = None
 
     @property
     def xi(self):
+        if self._xi is None:
+            self._xi = xifn(1., self._N)
         return self._xi
 
     # constants, float64 (wavelets.py:509-516, _gmw.py:191-195, 232-237)
@@ -299,6 +301,13 @@ class Wavelet():
             neg = np.sqrt(max(0., -2 * log_floor - mu**2))
             return (min(mu - r, -neg), mu + r)
         g, b, wc = k['gamma'], k['beta'], k['wc']
+        # memoized: the transforms build their wavelets per call
+        key = (self.kind, tuple(sorted(self.config.items())), float(log_floor))
+        hit = _BANDS.get(key)
+        if hit is not None:
+            return hit
+        if len(_BANDS) > 256:
+            _BANDS.clear()
         if self.poly() is not None:
             # a polynomial factor moves the peak: scan log|psih| on a fine
             # log grid and widen by a grid step on each side
@@ -307,7 +316,8 @@ class Wavelet():
                 lp = np.log(np.abs(self.fn(w)))
             keep = np.nonzero(lp >= lp.max() + log_floor)[0]
             i0, i1 = max(keep[0] - 1, 0), min(keep[-1] + 1, len(w) - 1)
-            return (float(w[i0]), float(w[i1]))
+            _BANDS[key] = (float(w[i0]), float(w[i1]))
+            return _BANDS[key]
 
         def e(w):  # log of psih relative to its peak at wc
             return b * np.log(w / wc) - (w**g - wc**g)
@@ -322,7 +332,8 @@ class Wavelet():
         for _ in range(200):
             mid = .5 * (lo + hi)
             lo, hi = (mid, hi) if e(mid) > log_floor else (lo, mid)
-        return (w_lo, hi)
+        _BANDS[key] = (w_lo, hi)
+        return _BANDS[key]
 
     def kernel_params(self):
         """(kind, p0, p1, p2, p3) passed to the CUDA kernels."""
@@ -335,6 +346,7 @@ class Wavelet():
 
 
 MAX_GMW_ORDER = 7
+_BANDS = {}   # (kind, config, log_floor) -> band of a GMW
 
 
 def _check_order(order):

@@ -316,10 +316,11 @@ def _grad_checks(astensor, rpadded, padtype):
 
 
 def _scales_out(r, astensor):
-    s = r['scales'].ravel().astype(r['dtype'])
     if astensor:
-        return torch.as_tensor(s, device=r['dev'])
-    return s
+        # a device-side cast of the cached float64 scales: no host copy, so
+        # the call stays asynchronous
+        return r['sc_d'].to(_RDT[r['dtype']], copy=True)
+    return r['scales'].ravel().astype(r['dtype'])
 
 
 def _check_ssq_args(squeezing, maprange, difftype, get_w=True, difforder=None):

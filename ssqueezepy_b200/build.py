@@ -52,8 +52,16 @@ def build(force=False, jobs=None, verbose=False):
     os.makedirs(OBJDIR, exist_ok=True)
     srcs = _sources()
 
+    # an object is reused when it is newer than its source and than every
+    # shared header (and this script); otherwise it is rebuilt
+    shared = [f for f in _deps() if not f.endswith('.cu')]
+    t_shared = max(os.path.getmtime(f) for f in shared)
+
     def compile_one(src):
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + '.o')
+        if (not force and os.path.exists(obj)
+                and os.path.getmtime(obj) >= max(os.path.getmtime(src), t_shared)):
+            return obj
         cmd = [NVCC, *ARCH, *FLAGS, '-I', INCLUDE, '-c', src, '-o', obj]
         if verbose:
             cmd.insert(1, '-Xptxas=-v')

@@ -10,9 +10,12 @@
 // backward sweep re-walks time from the end; at each step the last f whose
 // accumulated value matches within eps replaces the forward argmin. Sums are
 // rounded separately (no fused multiply-add) so they equal the reference's.
+#include <cooperative_groups.h>
 #include "launch.h"
 
 namespace ssqb {
+
+namespace cg = cooperative_groups;
 
 template <typename T> __device__ __forceinline__ T radd(T a, T b);
 template <> __device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
@@ -98,6 +101,188 @@ ridge_forward_kernel(const T* __restrict__ s, T penalty, int nf, int N, T* __res
   }
 }
 
+// ---- forward sweep over a thread-block cluster ------------------------------
+// CTA c of the cluster owns rows [c R, c R + R) (R = ceil(nf / kRidgeCluster));
+// K consecutive lanes share a row, lane k taking the candidates g = k, k+K, ...
+// and the K partial minima meet by shuffles. Every CTA holds the whole
+// previous column in shared memory, double-buffered: the lanes of a row
+// write its new value into the other buffer of every CTA through distributed
+// shared memory, and one cluster barrier (release / acquire) per time step
+// orders the steps. A candidate pen[g] + P[f, g] is NaN exactly when pen[g]
+// is (P is finite), so the NaN rule of the minimum becomes a per-column flag,
+// set by whoever writes a NaN, in three slots: read at step t, written at
+// t + 1, cleared for t + 2. With MAXC > 0 the lane's jump penalties
+// P[f, g] (constant in time) are computed once into registers.
+constexpr int kRidgeCluster = 8;
+
+template <typename T>
+__device__ __forceinline__ T tmin(T a, T b) { return b < a ? b : a; }
+
+template <typename T, int K, int MAXC>
+__global__ void __cluster_dims__(kRidgeCluster, 1, 1) __launch_bounds__(1024)
+ridge_forward_cluster_kernel(const T* __restrict__ s, T penalty, int nf, int N, int R,
+                             T* __restrict__ pen) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* prev = reinterpret_cast<T*>(smem_raw);  // [2][nf]
+  T* ss = prev + 2 * nf;                      // [nf]
+  __shared__ int nanflag[3];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int c = (int)cluster.block_rank();
+  const int tid = threadIdx.x;
+  const int k = tid % K;
+  const int fl = tid / K;
+  const int f = c * R + fl;
+  const bool active = fl < R && f < nf;
+  const unsigned gmask = (K == 32) ? 0xffffffffu
+                                   : (((1u << K) - 1u) << ((tid & 31) / K * K));
+  int has = 0;
+  for (int g = tid; g < nf; g += blockDim.x) {
+    const T v = pen[g];
+    prev[g] = v;
+    ss[g] = s[g];
+    has |= (v != v);
+  }
+  if (tid < 3) nanflag[tid] = 0;
+  has = __syncthreads_or(has);
+  if (tid == 0) nanflag[0] = has;
+  const T sf = active ? ss[f] : (T)0;
+  T P[MAXC > 0 ? MAXC : 1];
+  if (MAXC > 0) {
+#pragma unroll
+    for (int i = 0; i < (MAXC > 0 ? MAXC : 1); ++i) {
+      const int g = k + i * K;
+      P[i] = (active && g < nf) ? jump(penalty, sf, ss[g]) : (T)0;
+    }
+  }
+  cluster.sync();  // every CTA initialised before the first remote write
+  T e_next = (active && N > 1) ? pen[(size_t)nf + f] : (T)0;
+  for (int t = 1; t < N; ++t) {
+    const T* pv = prev + ((t - 1) & 1) * nf;
+    T* pw = prev + (t & 1) * nf;
+    const int col_nan = nanflag[(t - 1) % 3];
+    if (tid == 0) nanflag[(t + 1) % 3] = 0;
+    const T e_cur = e_next;
+    if (active && t + 1 < N) e_next = pen[(size_t)(t + 1) * nf + f];
+    if (active) {
+      T m0 = (T)INFINITY, m1 = (T)INFINITY;
+      if (MAXC > 0) {
+#pragma unroll
+        for (int i = 0; i < (MAXC > 0 ? MAXC : 1); i += 2) {
+          const int g0 = k + i * K, g1 = g0 + K;
+          if (g0 < nf) m0 = tmin(m0, radd(pv[g0], P[i]));
+          if (i + 1 < MAXC && g1 < nf) m1 = tmin(m1, radd(pv[g1], P[i + 1]));
+        }
+      } else {
+        int g = k;
+        for (; g + K < nf; g += 2 * K) {
+          m0 = tmin(m0, radd(pv[g], jump(penalty, sf, ss[g])));
+          m1 = tmin(m1, radd(pv[g + K], jump(penalty, sf, ss[g + K])));
+        }
+        if (g < nf) m0 = tmin(m0, radd(pv[g], jump(penalty, sf, ss[g])));
+      }
+      T m = tmin(m0, m1);
+#pragma unroll
+      for (int o = K / 2; o > 0; o >>= 1) m = tmin(m, __shfl_xor_sync(gmask, m, o));
+      if (col_nan) m = (T)NAN;
+      const T nv = radd(e_cur, m);
+      if (k == 0) pen[(size_t)t * nf + f] = nv;
+      const bool isnan_v = nv != nv;
+      for (int r = k; r < kRidgeCluster; r += K) {
+        *cluster.map_shared_rank(pw + f, r) = nv;
+        if (isnan_v) *cluster.map_shared_rank(&nanflag[t % 3], r) = 1;
+      }
+    }
+    cluster.sync();
+  }
+}
+
+// ---- backward sweep: one computing warp, rows staged in shared memory --------
+// Warp 0 walks time backwards; lane l holds s[f] for f = l + 32 i in registers
+// and reads the rows it needs from a shared-memory chunk of CH time steps
+// (pen and E, time-major) that all warps copy in before the chunk starts, the
+// next chunk's copy overlapping the walk of the current one.
+template <typename T, int I>
+__global__ void __launch_bounds__(256)
+ridge_backward_staged_kernel(const T* __restrict__ E, const T* __restrict__ pen,
+                             const T* __restrict__ s, T penalty, T eps, int nf, int N, int CH,
+                             int* __restrict__ ridge) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // two chunk buffers, each [CH + 1][nf] of pen then of E, and [CH] forward argmins
+  const size_t rows = (size_t)(CH + 1) * nf;
+  T* const base = reinterpret_cast<T*>(smem_raw);
+  int* const rbase = reinterpret_cast<int*>(base + 4 * rows);
+  // buffer b: pen rows at base + 2 b rows, E rows after them, argmins at rbase + b CH
+  const int tid = threadIdx.x, lane = tid & 31;
+  // chunk j covers steps t in [hi_j - CH + 1, hi_j], hi_j = N - 2 - j CH, plus
+  // row hi_j + 1 (the step above it)
+  // copied by threads q0, q0 + 1, ... of the block (all of them before the
+  // walk starts, warps 1.. while warp 0 walks)
+  auto stage = [&](int j, int b, int q0) {
+    const int qt = tid - q0, qs = blockDim.x - q0;
+    const int hi = N - 2 - j * CH;
+    const int lo = hi - CH + 1 < 0 ? 0 : hi - CH + 1;
+    const int n_rows = hi + 1 - lo + 1;  // rows lo .. hi + 1
+    const size_t n = (size_t)n_rows * nf;
+    const T* gp = pen + (size_t)lo * nf;
+    const T* ge = E + (size_t)lo * nf;
+    T* sp = base + 2 * (size_t)b * rows;
+    T* se = sp + rows;
+    int* sr = rbase + b * CH;
+    for (size_t q = qt; q < n; q += qs) {
+      sp[q] = gp[q];
+      se[q] = ge[q];
+    }
+    for (int q = qt; q < hi + 1 - lo; q += qs) sr[q] = ridge[lo + q];
+  };
+  T sreg[I];
+#pragma unroll
+  for (int i = 0; i < I; ++i) {
+    const int f = lane + 32 * i;
+    sreg[i] = f < nf ? s[f] : (T)0;
+  }
+  const int nchunks = (N - 1 + CH - 1) / CH;
+  int r = ridge[N - 1];
+  r = r < 0 ? 0 : (r >= nf ? nf - 1 : r);
+  if (nchunks > 0) stage(0, 0, 0);
+  __syncthreads();
+  for (int j = 0; j < nchunks; ++j) {
+    const int b = j & 1;
+    if (tid >= 32) {
+      if (j + 1 < nchunks) stage(j + 1, b ^ 1, 32);
+    } else {
+      const int hi = N - 2 - j * CH;
+      const int lo = hi - CH + 1 < 0 ? 0 : hi - CH + 1;
+      const T* P = base + 2 * (size_t)b * rows;
+      const T* Eb = P + rows;
+      const int* Rb = rbase + b * CH;
+      for (int t = hi; t >= lo; --t) {
+        const T* prow = P + (size_t)(t - lo) * nf;         // pen[t, :]
+        const size_t o = (size_t)(t + 1 - lo) * nf + r;    // (t + 1, r)
+        const T val = rsub(P[o], Eb[o]);
+        T sr = (T)0;
+#pragma unroll
+        for (int i = 0; i < I; ++i)
+          if (i == (r >> 5)) sr = sreg[i];
+        sr = __shfl_sync(0xffffffffu, sr, r & 31);
+        int best = -1;
+#pragma unroll
+        for (int i = 0; i < I; ++i) {
+          const int f = lane + 32 * i;
+          if (f < nf) {
+            const T d = rsub(val, radd(prow[f], jump(penalty, sr, sreg[i])));
+            if (fabs(d) < eps) best = f;
+          }
+        }
+        best = __reduce_max_sync(0xffffffffu, best);
+        int rt = best >= 0 ? best : Rb[t - lo];
+        if (lane == 0 && best >= 0) ridge[t] = best;
+        r = rt < 0 ? 0 : (rt >= nf ? nf - 1 : rt);  // in range by construction
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // per column: first index of the minimum over f (the first NaN if any)
 template <typename T>
 __global__ void ridge_argmin_kernel(const T* __restrict__ pen, int nf, int N,
@@ -173,6 +358,75 @@ __global__ void ridge_finish_kernel(const int* __restrict__ ridge, const T* __re
   for (long long f = a; f < b; ++f) energy[(size_t)f * N + t] = (T)0;
 }
 
+template <typename T, int K, int MAXC>
+static cudaError_t launch_fwd_cluster(const T* s, T penalty, int nf, int N, T* pen,
+                                      cudaStream_t st) {
+  const int R = (nf + kRidgeCluster - 1) / kRidgeCluster;
+  const int threads = ((R * K + 31) / 32) * 32;
+  const size_t smem = 3 * (size_t)nf * sizeof(T);
+  auto k = ridge_forward_cluster_kernel<T, K, MAXC>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  k<<<kRidgeCluster, threads, smem, st>>>(s, penalty, nf, N, R, pen);
+  return cudaGetLastError();
+}
+
+// the cluster sweep for up to 1024 rows per CTA; larger nf keeps the
+// single-CTA sweep
+template <typename T>
+static cudaError_t launch_ridge_forward(const T* s, T penalty, int nf, int N, T* pen,
+                                        cudaStream_t st) {
+  const int R = (nf + kRidgeCluster - 1) / kRidgeCluster;
+  if (3 * (size_t)nf * sizeof(T) <= 200 * 1024) {
+    if (R * 16 <= 1024 && (nf + 15) / 16 <= 32)
+      return launch_fwd_cluster<T, 16, 32>(s, penalty, nf, N, pen, st);
+    if (R * 8 <= 1024) return launch_fwd_cluster<T, 8, 0>(s, penalty, nf, N, pen, st);
+    if (R * 4 <= 1024) return launch_fwd_cluster<T, 4, 0>(s, penalty, nf, N, pen, st);
+    if (R <= 1024) return launch_fwd_cluster<T, 1, 0>(s, penalty, nf, N, pen, st);
+  }
+  const size_t smem = 2 * (size_t)nf * sizeof(T);
+  auto fk = ridge_forward_kernel<T>;
+  cudaError_t e = cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  fk<<<1, 1024, smem, st>>>(s, penalty, nf, N, pen);
+  return cudaGetLastError();
+}
+
+template <typename T, int I>
+static cudaError_t launch_bwd_staged(const T* E, const T* pen, const T* s, T penalty, T eps,
+                                     int nf, int N, int CH, size_t smem, int* ridge,
+                                     cudaStream_t st) {
+  auto k = ridge_backward_staged_kernel<T, I>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  k<<<1, 256, smem, st>>>(E, pen, s, penalty, eps, nf, N, CH, ridge);
+  return cudaGetLastError();
+}
+
+// staged single-warp walk for nf <= 1024 (32 rows per lane at most) when a
+// chunk of at least 4 steps fits; else the block-wide walk
+template <typename T>
+static cudaError_t launch_ridge_backward(const T* E, const T* pen, const T* s, T penalty, T eps,
+                                         int nf, int N, int* ridge, cudaStream_t st) {
+  if (N < 2) return cudaSuccess;
+  const size_t per_step = 2 * 2 * (size_t)nf * sizeof(T) + 2 * sizeof(int);
+  const size_t budget = 160 * 1024;
+  int CH = (int)((budget - 2 * 2 * (size_t)nf * sizeof(T)) / per_step);
+  if (CH > 64) CH = 64;
+  if (nf <= 1024 && CH >= 4) {
+    const size_t smem = 2 * 2 * (size_t)(CH + 1) * nf * sizeof(T) + 2 * (size_t)CH * sizeof(int);
+    if (nf <= 128) return launch_bwd_staged<T, 4>(E, pen, s, penalty, eps, nf, N, CH, smem, ridge, st);
+    if (nf <= 320) return launch_bwd_staged<T, 10>(E, pen, s, penalty, eps, nf, N, CH, smem, ridge, st);
+    if (nf <= 512) return launch_bwd_staged<T, 16>(E, pen, s, penalty, eps, nf, N, CH, smem, ridge, st);
+    return launch_bwd_staged<T, 32>(E, pen, s, penalty, eps, nf, N, CH, smem, ridge, st);
+  }
+  ridge_backward_kernel<T><<<1, 1024, 0, st>>>(E, pen, s, penalty, eps, nf, N, ridge);
+  return cudaGetLastError();
+}
+
 template <typename C>
 static int run_ridges_t(const C* Tf, int nf, int N, const void* s, const void* scales,
                         double penalty, int n_ridges, int bw, double eps, int* idx_out,
@@ -187,17 +441,14 @@ static int run_ridges_t(const C* Tf, int nf, int N, const void* s, const void* s
   ridge_energy_kernel<C><<<(unsigned)((n + nt - 1) / nt), nt, 0, st>>>(Tf, n, energy);
   cudaError_t e = cudaGetLastError();
   if (e) return e;
-  const size_t smem = 2 * (size_t)nf * sizeof(T);
-  auto fk = ridge_forward_kernel<T>;
-  if ((e = cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-    return e;
   const unsigned gN = (unsigned)((N + nt - 1) / nt);
   for (int i = 0; i < n_ridges; ++i) {
     ridge_prep_kernel<T><<<gN, nt, 0, st>>>(energy, nf, N, (T)eps, E, pen);
-    fk<<<1, 1024, smem, st>>>((const T*)s, (T)penalty, nf, N, pen);
+    if ((e = launch_ridge_forward<T>((const T*)s, (T)penalty, nf, N, pen, st))) return e;
     ridge_argmin_kernel<T><<<gN, nt, 0, st>>>(pen, nf, N, ridge);
-    ridge_backward_kernel<T><<<1, 1024, 0, st>>>(E, pen, (const T*)s, (T)penalty, (T)eps, nf,
-                                                 N, ridge);
+    if ((e = launch_ridge_backward<T>(E, pen, (const T*)s, (T)penalty, (T)eps, nf, N, ridge,
+                                      st)))
+      return e;
     ridge_finish_kernel<T><<<gN, nt, 0, st>>>(ridge, (const T*)scales, nf, N, bw, i, n_ridges,
                                               energy, idx_out, (T*)f_out, (T*)e_out);
     if ((e = cudaGetLastError())) return e;
