@@ -105,14 +105,17 @@ ridge_forward_kernel(const T* __restrict__ s, T penalty, int nf, int N, T* __res
 // CTA c of the cluster owns rows [c R, c R + R) (R = ceil(nf / kRidgeCluster));
 // K consecutive lanes share a row, lane k taking the candidates g = k, k+K, ...
 // and the K partial minima meet by shuffles. Every CTA holds the whole
-// previous column in shared memory, double-buffered: the lanes of a row
-// write its new value into the other buffer of every CTA through distributed
-// shared memory, and one cluster barrier (release / acquire) per time step
-// orders the steps. A candidate pen[g] + P[f, g] is NaN exactly when pen[g]
-// is (P is finite), so the NaN rule of the minimum becomes a per-column flag,
-// set by whoever writes a NaN, in three slots: read at step t, written at
-// t + 1, cleared for t + 2. With MAXC > 0 the lane's jump penalties
-// P[f, g] (constant in time) are computed once into registers.
+// previous column in shared memory, double-buffered: lanes of a row write its
+// new value into the other buffer of every CTA through distributed shared
+// memory, and one cluster barrier per time step orders the steps. A candidate
+// pen[g] + P[f, g] is NaN exactly when pen[g] is (P is finite), so the NaN rule
+// of the minimum becomes a per-column flag, set by whoever writes a NaN, in
+// three slots: read at step t, written at t + 1, cleared for t + 2. With
+// MAXC > 0 the lane's jump penalties P[f, g] (constant in time) sit in
+// registers. Global memory stays out of the steps: the barrier's release
+// would wait for every outstanding global access, so E for the CTA's rows is
+// read into shared memory CHF steps at a time and the accumulated values are
+// collected there and written back once per chunk.
 constexpr int kRidgeCluster = 8;
 
 template <typename T>
@@ -121,18 +124,22 @@ __device__ __forceinline__ T tmin(T a, T b) { return b < a ? b : a; }
 template <typename T, int K, int MAXC>
 __global__ void __cluster_dims__(kRidgeCluster, 1, 1) __launch_bounds__(1024)
 ridge_forward_cluster_kernel(const T* __restrict__ s, T penalty, int nf, int N, int R,
-                             T* __restrict__ pen) {
+                             int CHF, T* __restrict__ pen) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* prev = reinterpret_cast<T*>(smem_raw);  // [2][nf]
   T* ss = prev + 2 * nf;                      // [nf]
+  T* eb = ss + nf;                            // [CHF][R]  E of this chunk's steps
+  T* ob = eb + (size_t)CHF * R;               // [CHF][R]  accumulated values
   __shared__ int nanflag[3];
   cg::cluster_group cluster = cg::this_cluster();
   const int c = (int)cluster.block_rank();
   const int tid = threadIdx.x;
   const int k = tid % K;
   const int fl = tid / K;
-  const int f = c * R + fl;
-  const bool active = fl < R && f < nf;
+  const int f0 = c * R;
+  const int f = f0 + fl;
+  const int rows = (nf - f0) < R ? (nf - f0 > 0 ? nf - f0 : 0) : R;  // rows owned
+  const bool active = fl < rows;
   const unsigned gmask = (K == 32) ? 0xffffffffu
                                    : (((1u << K) - 1u) << ((tid & 31) / K * K));
   int has = 0;
@@ -155,45 +162,82 @@ ridge_forward_cluster_kernel(const T* __restrict__ s, T penalty, int nf, int N, 
     }
   }
   cluster.sync();  // every CTA initialised before the first remote write
-  T e_next = (active && N > 1) ? pen[(size_t)nf + f] : (T)0;
-  for (int t = 1; t < N; ++t) {
-    const T* pv = prev + ((t - 1) & 1) * nf;
-    T* pw = prev + (t & 1) * nf;
-    const int col_nan = nanflag[(t - 1) % 3];
-    if (tid == 0) nanflag[(t + 1) % 3] = 0;
-    const T e_cur = e_next;
-    if (active && t + 1 < N) e_next = pen[(size_t)(t + 1) * nf + f];
-    if (active) {
-      T m0 = (T)INFINITY, m1 = (T)INFINITY;
-      if (MAXC > 0) {
-#pragma unroll
-        for (int i = 0; i < (MAXC > 0 ? MAXC : 1); i += 2) {
-          const int g0 = k + i * K, g1 = g0 + K;
-          if (g0 < nf) m0 = tmin(m0, radd(pv[g0], P[i]));
-          if (i + 1 < MAXC && g1 < nf) m1 = tmin(m1, radd(pv[g1], P[i + 1]));
-        }
-      } else {
-        int g = k;
-        for (; g + K < nf; g += 2 * K) {
-          m0 = tmin(m0, radd(pv[g], jump(penalty, sf, ss[g])));
-          m1 = tmin(m1, radd(pv[g + K], jump(penalty, sf, ss[g + K])));
-        }
-        if (g < nf) m0 = tmin(m0, radd(pv[g], jump(penalty, sf, ss[g])));
-      }
-      T m = tmin(m0, m1);
-#pragma unroll
-      for (int o = K / 2; o > 0; o >>= 1) m = tmin(m, __shfl_xor_sync(gmask, m, o));
-      if (col_nan) m = (T)NAN;
-      const T nv = radd(e_cur, m);
-      if (k == 0) pen[(size_t)t * nf + f] = nv;
-      const bool isnan_v = nv != nv;
-      for (int r = k; r < kRidgeCluster; r += K) {
-        *cluster.map_shared_rank(pw + f, r) = nv;
-        if (isnan_v) *cluster.map_shared_rank(&nanflag[t % 3], r) = 1;
-      }
+  // lanes that write other CTAs' buffers: 1..C when a row has more lanes than
+  // the cluster has CTAs (lane 0 keeps the chunk store), else all lanes
+  const bool remote_lane = (K > kRidgeCluster) ? (k >= 1 && k <= kRidgeCluster) : true;
+  for (int t0 = 1; t0 < N; t0 += CHF) {
+    const int nst = (N - t0) < CHF ? (N - t0) : CHF;
+    // read E[t0 .. t0 + nst) for the owned rows (pen still holds E there)
+    for (int q = tid; q < nst * rows; q += blockDim.x) {
+      const int tt = q / rows, r = q % rows;
+      eb[tt * R + r] = pen[(size_t)(t0 + tt) * nf + f0 + r];
     }
-    cluster.sync();
+    __syncthreads();
+    for (int tt = 0; tt < nst; ++tt) {
+      const int t = t0 + tt;
+      const T* pv = prev + ((t - 1) & 1) * nf;
+      T* pw = prev + (t & 1) * nf;
+      const int col_nan = nanflag[(t - 1) % 3];
+      if (tid == 0) nanflag[(t + 1) % 3] = 0;
+      if (active) {
+        T m0 = (T)INFINITY, m1 = (T)INFINITY;
+        if (MAXC > 0) {
+#pragma unroll
+          for (int i = 0; i < (MAXC > 0 ? MAXC : 1); i += 2) {
+            const int g0 = k + i * K, g1 = g0 + K;
+            if (g0 < nf) m0 = tmin(m0, radd(pv[g0], P[i]));
+            if (i + 1 < MAXC && g1 < nf) m1 = tmin(m1, radd(pv[g1], P[i + 1]));
+          }
+        } else {
+          int g = k;
+          for (; g + K < nf; g += 2 * K) {
+            m0 = tmin(m0, radd(pv[g], jump(penalty, sf, ss[g])));
+            m1 = tmin(m1, radd(pv[g + K], jump(penalty, sf, ss[g + K])));
+          }
+          if (g < nf) m0 = tmin(m0, radd(pv[g], jump(penalty, sf, ss[g])));
+        }
+        T m = tmin(m0, m1);
+#pragma unroll
+        for (int o = K / 2; o > 0; o >>= 1) m = tmin(m, __shfl_xor_sync(gmask, m, o));
+        if (col_nan) m = (T)NAN;
+        const T nv = radd(eb[tt * R + fl], m);
+        if (k == 0) ob[tt * R + fl] = nv;
+        const bool isnan_v = nv != nv;
+        if (K > kRidgeCluster) {
+          if (remote_lane) {
+            const int r = k - 1;
+            *cluster.map_shared_rank(pw + f, r) = nv;
+            if (isnan_v) *cluster.map_shared_rank(&nanflag[t % 3], r) = 1;
+          }
+        } else {
+          for (int r = k; r < kRidgeCluster; r += K) {
+            *cluster.map_shared_rank(pw + f, r) = nv;
+            if (isnan_v) *cluster.map_shared_rank(&nanflag[t % 3], r) = 1;
+          }
+        }
+      }
+      cluster.sync();  // every thread of the cluster, every step
+    }
+    // write the chunk's accumulated values back (ob complete: the last
+    // cluster barrier also ordered the CTA's own threads)
+    for (int q = tid; q < nst * rows; q += blockDim.x) {
+      const int tt = q / rows, r = q % rows;
+      pen[(size_t)(t0 + tt) * nf + f0 + r] = ob[tt * R + r];
+    }
+    __syncthreads();  // eb / ob are rewritten by the next chunk
   }
+}
+
+// asynchronous global -> shared copy of one 4- or 8-byte element (cp.async:
+// the copy does not pass through registers, so a thread's copies overlap)
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (sizeof(T) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(d), "l"(src) : "memory");
 }
 
 // ---- backward sweep: one computing warp, rows staged in shared memory --------
@@ -229,10 +273,11 @@ ridge_backward_staged_kernel(const T* __restrict__ E, const T* __restrict__ pen,
     T* se = sp + rows;
     int* sr = rbase + b * CH;
     for (size_t q = qt; q < n; q += qs) {
-      sp[q] = gp[q];
-      se[q] = ge[q];
+      cp_async_elem(sp + q, gp + q);
+      cp_async_elem(se + q, ge + q);
     }
-    for (int q = qt; q < hi + 1 - lo; q += qs) sr[q] = ridge[lo + q];
+    for (int q = qt; q < hi + 1 - lo; q += qs) cp_async_elem(sr + q, ridge + lo + q);
+    asm volatile("cp.async.commit_group;" ::: "memory");
   };
   T sreg[I];
 #pragma unroll
@@ -244,11 +289,13 @@ ridge_backward_staged_kernel(const T* __restrict__ E, const T* __restrict__ pen,
   int r = ridge[N - 1];
   r = r < 0 ? 0 : (r >= nf ? nf - 1 : r);
   if (nchunks > 0) stage(0, 0, 0);
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
   for (int j = 0; j < nchunks; ++j) {
     const int b = j & 1;
     if (tid >= 32) {
       if (j + 1 < nchunks) stage(j + 1, b ^ 1, 32);
+      asm volatile("cp.async.wait_all;" ::: "memory");
     } else {
       const int hi = N - 2 - j * CH;
       const int lo = hi - CH + 1 < 0 ? 0 : hi - CH + 1;
@@ -358,27 +405,40 @@ __global__ void ridge_finish_kernel(const int* __restrict__ ridge, const T* __re
   for (long long f = a; f < b; ++f) energy[(size_t)f * N + t] = (T)0;
 }
 
+constexpr size_t kRidgeFwdSmem = 200 * 1024;
+
+// steps per chunk of the cluster sweep: up to 64, as shared memory allows
+template <typename T>
+static int fwd_chunk(int nf, int R) {
+  const size_t fixed = 3 * (size_t)nf * sizeof(T);
+  if (fixed >= kRidgeFwdSmem) return 0;
+  const size_t per = 2 * (size_t)R * sizeof(T);
+  const size_t c = (kRidgeFwdSmem - fixed) / per;
+  return c >= 64 ? 64 : (int)c;
+}
+
 template <typename T, int K, int MAXC>
 static cudaError_t launch_fwd_cluster(const T* s, T penalty, int nf, int N, T* pen,
                                       cudaStream_t st) {
   const int R = (nf + kRidgeCluster - 1) / kRidgeCluster;
   const int threads = ((R * K + 31) / 32) * 32;
-  const size_t smem = 3 * (size_t)nf * sizeof(T);
+  const int CHF = fwd_chunk<T>(nf, R);
+  const size_t smem = (3 * (size_t)nf + 2 * (size_t)CHF * R) * sizeof(T);
   auto k = ridge_forward_cluster_kernel<T, K, MAXC>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e) return e;
-  k<<<kRidgeCluster, threads, smem, st>>>(s, penalty, nf, N, R, pen);
+  k<<<kRidgeCluster, threads, smem, st>>>(s, penalty, nf, N, R, CHF, pen);
   return cudaGetLastError();
 }
 
-// the cluster sweep for up to 1024 rows per CTA; larger nf keeps the
-// single-CTA sweep
+// the cluster sweep for up to 1024 rows per CTA with room for a chunk of at
+// least 8 steps; otherwise the single-CTA sweep
 template <typename T>
 static cudaError_t launch_ridge_forward(const T* s, T penalty, int nf, int N, T* pen,
                                         cudaStream_t st) {
   const int R = (nf + kRidgeCluster - 1) / kRidgeCluster;
-  if (3 * (size_t)nf * sizeof(T) <= 200 * 1024) {
+  if (fwd_chunk<T>(nf, R) >= 8) {
     if (R * 16 <= 1024 && (nf + 15) / 16 <= 32)
       return launch_fwd_cluster<T, 16, 32>(s, penalty, nf, N, pen, st);
     if (R * 8 <= 1024) return launch_fwd_cluster<T, 8, 0>(s, penalty, nf, N, pen, st);
