@@ -289,18 +289,35 @@ def run_ours(args):
 
 
 def run_e2e(sb, torch, dist, x_np, na, N, st, world, dev, barrier, args):
+    """The headline metric through the public API from host buffers: every
+    step copies its signal from pinned host memory to the device, runs
+    ssq_cwt and copies Tx (na x N complex64) back to pinned host memory. Steps
+    alternate between two streams, as a streaming caller would, so one step's
+    copy back overlaps the next step's transform; the region ends when every
+    step's copy back has finished."""
     x_pin = torch.from_numpy(x_np).pin_memory()
-    Tx_pin = torch.empty((na, N), dtype=torch.complex64).pin_memory()
-    for _ in range(2):
-        Tp, *_ = sb.ssq_cwt(x_pin, WAVELET, scales='log-piecewise', nv=32)
-        Tx_pin.copy_(Tp, non_blocking=True)
+    Tx_pin = [torch.empty((na, N), dtype=torch.complex64).pin_memory() for _ in range(2)]
+    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+
+    def step(k):
+        s = streams[k % 2]
+        with torch.cuda.stream(s):
+            Tp, *_ = sb.ssq_cwt(x_pin, WAVELET, scales='log-piecewise', nv=32)
+            Tx_pin[k % 2].copy_(Tp, non_blocking=True)
+
+    for k in range(2):
+        step(k)
+    torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = max(4, min(args.steps, 10))
     e0.record(st)
-    for _ in range(e2e_steps):
-        Tp, *_ = sb.ssq_cwt(x_pin, WAVELET, scales='log-piecewise', nv=32)
-        Tx_pin.copy_(Tp, non_blocking=True)
+    for s in streams:
+        s.wait_event(e0)
+    for k in range(e2e_steps):
+        step(k)
+    for s in streams:
+        st.wait_stream(s)
     e1.record(st)
     barrier()
     e2e_ms, = max_over_ranks([e0.elapsed_time(e1) / e2e_steps], dev)
@@ -671,7 +688,10 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
                          "path_frac": alg_total / (step_ms_max * 1e-3) / 1e9 / hbm},
             "e2e": (None if e2e_value is None else
                     {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * N,
-                     "d2h_bytes_per_step": 8 * na * N}),
+                     "d2h_bytes_per_step": 8 * na * N,
+                     "schedule": "public API from pinned host memory, steps alternating "
+                                 "over two streams (a step's copy back overlaps the next "
+                                 "step's transform)"}),
             "gpu_launches": launches * args.steps,
             "clocks": clocks,
         }
