@@ -67,6 +67,27 @@ def peaks():
         return 6650.0, 'fallback'
 
 
+def fp64_peak_tflops(torch, dev):
+    """Measured float64 throughput of this GPU: cuBLAS DGEMM 4096^3 (2 N^3
+    flops), best of 5 after a warm-up, CUDA events. The denominator of the
+    CWT kernel's compute roofline (its float64 FFTs), measured here because
+    the peak file holds HBM and bf16 figures only."""
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = float('inf')
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
 class Clocks:
     """nvidia-smi sampler running during the timed region."""
     Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
@@ -232,6 +253,7 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    fp64_tf = fp64_peak_tflops(torch, dev) if rank == 0 else None
     clk = Clocks(local) if rank == 0 else None  # samples through every timed leg
     for _ in range(max(args.warmup, 3)):
         step()
@@ -281,7 +303,7 @@ def run_ours(args):
     if rank == 0:
         emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
              launches, clocks, sc, f, const, Tx_keep, Wx_keep, batched, train, long_,
-             stft_, next_)
+             stft_, next_, fp64_tf)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -654,7 +676,7 @@ def run_long(args, torch, dev, world, barrier):
 
 def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
          launches, clocks, sc, f, const, Tg, Wg, batched=None, train=None, long_=None,
-         stft_=None, next_=None):
+         stft_=None, next_=None, fp64_tf=None):
     hbm, src = peaks()
     if True:
         alg_cwt = (4 + 8 * na) * N          # read x, write Wx
@@ -686,6 +708,16 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
                                            "(row, sample), scaled to this call",
                          "peak_source": src,
                          "path_frac": alg_total / (step_ms_max * 1e-3) / 1e9 / hbm},
+            "compute_roofline": None if fp64_tf is None else {
+                "kernel": "cwt", "bound": "fp64",
+                "flops_per_call": 10.0 * Npad * np.log2(Npad) * na,
+                "flop_count": "2 complex inverse FFTs of Npad per row, 5 Npad log2 Npad "
+                              "each (radix-2 count); wavelet, twiddle and phase-transform "
+                              "arithmetic not counted",
+                "achieved": 10.0 * Npad * np.log2(Npad) * na / (cwt_avg * 1e-3) / 1e12,
+                "peak": fp64_tf, "unit": "TFLOP/s",
+                "frac": 10.0 * Npad * np.log2(Npad) * na / (cwt_avg * 1e-3) / 1e12 / fp64_tf,
+                "peak_source": "measured here: cuBLAS float64 GEMM 4096^3"},
             "e2e": (None if e2e_value is None else
                     {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * N,
                      "d2h_bytes_per_step": 8 * na * N,
