@@ -10,7 +10,8 @@ frequencies, bin mapping); there is no CPU fallback.
 from ._transforms import (cwt, ssq_cwt, icwt, stft, istft, ssq_stft, ssqueeze,
                           phase_cwt, phase_cwt_num, phase_stft, issq_cwt, issq_stft, Wavelet,
                           configure)
-from ._params import (p2up, process_scales, make_scales, cwt_scalebounds,
+from ._params import get_window_public as get_window
+from ._params import (p2up, padsignal, process_scales, make_scales, cwt_scalebounds,
                       center_frequency, adm_ssq, logscale_transition_idx,
                       infer_scaletype, nv_from_scales)
 from ._batch import SsqCwtBatch, ssq_cwt_batch
@@ -18,7 +19,8 @@ from ._ridges import extract_ridges
 from . import _lib
 
 __version__ = '0.1.0'
-__all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'istft', 'ssq_stft', 'ssqueeze',
+__all__ = ['cwt', 'ssq_cwt', 'icwt', 'stft', 'istft', 'ssq_stft', 'ssqueeze', 'get_window',
+           'padsignal',
            'phase_cwt', 'phase_cwt_num', 'phase_stft', 'Wavelet', 'configure', 'p2up', 'process_scales',
            'make_scales', 'cwt_scalebounds', 'center_frequency', 'adm_ssq',
            'logscale_transition_idx', 'infer_scaletype', 'nv_from_scales',

@@ -879,6 +879,56 @@ def get_window(window, win_len, n_fft=None, derivative=False):
     return window, diff_window
 
 
+def get_window_public(window, win_len, n_fft=None, derivative=False, dtype=None):
+    """`get_window` of _stft.py:259-310: the window padded to `n_fft` (and its
+    frequency-domain derivative), cast to `dtype` (default: float64, the
+    window's own) with denormals zeroed."""
+    if isinstance(window, np.ndarray) and len(window) != win_len:
+        import warnings
+        warnings.warn("len(window) != win_len (%s != %s)" % (len(window), win_len))
+    win, dwin = get_window(window, win_len, n_fft, derivative=derivative)
+    dt = _dtype_str(dtype) if dtype is not None else 'float64'
+    win = zero_denormals(win.astype(dt))
+    if derivative:
+        return win, zero_denormals(dwin.astype(dt))
+    return win
+
+
+def padsignal(x, padtype='reflect', padlength=None, get_params=False):
+    """`padsignal` of utils/common.py:54-158: pad the last axis of a 1D / 2D
+    numpy array or torch tensor to `padlength` (default: `p2up`), left pad n1,
+    right pad n2. numpy arrays take all five modes on the host (np.pad, and
+    the edge-repeating 'symmetric' by reversal); tensors take 'zero' and
+    'reflect' on their device, as the reference allows."""
+    is_numpy = isinstance(x, np.ndarray)
+    supported = (('zero', 'reflect', 'symmetric', 'replicate', 'wrap') if is_numpy
+                 else ('zero', 'reflect'))
+    if padtype not in supported:
+        raise ValueError("`padtype` must be one of: %s (got %s)"
+                         % (', '.join(supported), padtype))
+    if not hasattr(x, 'ndim'):
+        raise TypeError("`x` must be a numpy array or torch Tensor (got %s)" % type(x))
+    if x.ndim not in (1, 2):
+        raise ValueError("`x` must be 1D or 2D (got x.ndim == %s)" % x.ndim)
+    n_up, n1, n2 = pad_geometry(x.shape[-1], padlength)
+    if is_numpy:
+        pw = (n1, n2) if x.ndim == 1 else [(0, 0), (n1, n2)]
+        if padtype == 'symmetric':
+            r = x[..., ::-1]
+            xp = np.concatenate([r[..., r.shape[-1] - n1:] if n1 else r[..., :0], x,
+                                 r[..., :n2]], axis=-1)
+        else:
+            mode = {'zero': 'constant', 'reflect': 'reflect', 'replicate': 'edge',
+                    'wrap': 'wrap'}[padtype]
+            xp = np.pad(x, pw, mode=mode)
+    else:
+        import torch
+        mode = 'constant' if padtype == 'zero' else 'reflect'
+        xp = (torch.nn.functional.pad(x[None], (n1, n2), mode)[0] if x.ndim == 1 else
+              torch.nn.functional.pad(x, (n1, n2), mode))
+    return (xp, n_up, n1, n2) if get_params else xp
+
+
 def zero_denormals(x):
     """Zero |x| < 1000*tiny (algos.py:593-612)."""
     tiny = 1000 * np.finfo(x.dtype).tiny

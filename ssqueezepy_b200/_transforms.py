@@ -326,15 +326,12 @@ def _scales_out(r, astensor):
 def _check_ssq_args(squeezing, maprange, difftype, get_w=True, difforder=None):
     """The argument checks of ssqueezing.py:314-368; returns `difforder`
     (4 by default for difftype='numeric')."""
-    if not isinstance(squeezing, str):
-        raise NotImplementedError("custom `squeezing` functions are not on the "
-                                  "accelerated path")
-    if squeezing not in ('sum', 'lebesgue', 'abs'):
+    if not (isinstance(squeezing, str) or callable(squeezing)):
+        raise TypeError("`squeezing` must be string or function "
+                        "(got %s)" % type(squeezing))
+    if isinstance(squeezing, str) and squeezing not in ('sum', 'lebesgue', 'abs'):
         raise ValueError("`squeezing` must be one of: sum, lebesgue, abs "
                          "(got %s)" % squeezing)
-    if squeezing != 'sum':
-        raise NotImplementedError("only squeezing='sum' is on the accelerated "
-                                  "path")
     if isinstance(maprange, (tuple, list)):
         if not all(isinstance(m, (float, int)) for m in maprange):
             raise ValueError("all elements of `maprange` must be float or int")
@@ -359,6 +356,44 @@ def _check_ssq_args(squeezing, maprange, difftype, get_w=True, difforder=None):
     elif difftype == 'numeric':
         difforder = 4
     return difforder
+
+
+def _squeeze_values(W, squeezing):
+    """The values the squeeze sums (ssqueezing.py:196-201): Wx itself for
+    'sum', `ones / len(Wx)` for 'lebesgue' (len: the first axis of Wx as the
+    caller shaped it), |Wx| for 'abs', or `squeezing(Wx)` for a function (on
+    the device tensor). With no `w` given, the reference also takes the phase
+    transform from these values and dWx, and so does the squeeze here."""
+    if callable(squeezing):
+        out = torch.as_tensor(squeezing(W)).to(device=W.device, dtype=W.dtype)
+        if out.shape != W.shape:
+            raise ValueError("`squeezing` function must keep the shape of Wx")
+        return out.contiguous()
+    if squeezing == 'lebesgue':
+        return torch.full_like(W, 1. / W.shape[0])
+    if squeezing == 'abs':
+        return W.abs().to(W.dtype)
+    return W
+
+
+def _squeeze_from(Wv, w, dW, sfs_d, cst, mode, bp, nbins, flipud, gamma):
+    """Tx from squeeze values Wv (B, na, N) and either a phase transform w
+    (`ssqb_indexed_sum`) or dWx for the phase on the fly
+    (`ssqb_ssqueeze_fast`)."""
+    B, na, N = Wv.shape
+    prec = L.F64 if Wv.dtype == torch.complex128 else L.F32
+    Tx = torch.empty_like(Wv)
+    cb = L.make_bins(mode, bp, nbins, flipud)
+    with torch.cuda.device(Wv.device):
+        if w is not None:
+            rc = L.load().ssqb_indexed_sum(L.ptr(Wv), L.ptr(w.contiguous()), L.ptr(cst), cb,
+                                           B, na, N, prec, L.ptr(Tx), L.stream_ptr())
+        else:
+            rc = L.load().ssqb_ssqueeze_fast(L.ptr(Wv), L.ptr(dW.contiguous()), L.ptr(sfs_d),
+                                             L.ptr(cst), cb, float(gamma), B, na, N, prec,
+                                             L.ptr(Tx), L.stream_ptr())
+    L.check(rc, 'ssqueeze')
+    return Tx
 
 
 def _ssq_freqs_for_cwt(ssq_freqs, scales, N, wavelet, cwt_scaletype, maprange,
@@ -436,7 +471,29 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
     if difftype != 'trig':
         return _ssq_cwt_by_differences(
             x, wavelet, kernel, scales, nv, fs, t, dt, padtype, nan_checks, gamma, sp,
-            ssq_freqs, maprange, flipud, difftype, difforder, astensor, get_dWx)
+            ssq_freqs, maprange, flipud, difftype, difforder, astensor, get_dWx,
+            squeezing)
+    if not (isinstance(squeezing, str) and squeezing == 'sum'):
+        # the squeeze sums other values than Wx (ssqueezing.py:196-201): Wx
+        # and dWx (or w) first, then the squeeze from the replaced values
+        if A.needs_grad(x):
+            raise NotImplementedError("gradients need squeezing='sum'")
+        fp = _ssq_plan(wavelet, scales, N, nv, ssq_freqs, maprange, padtype, dt, sp)
+        r = _cwt_core(x, wavelet, scales, nv, fs, t, padtype, False, nan_checks, True,
+                      want_w=get_w, gamma=gamma, kernel=kernel)
+        is2 = r['is_2d']
+        W3 = r['Wx']
+        Wv = _squeeze_values(W3 if is2 else W3[0], squeezing)
+        Wv = Wv if is2 else Wv[None]
+        Tx = _squeeze_from(Wv, r['w'], r['dWx'], None, _on_device(fp, 'const', r['dev']),
+                           fp['mode'], fp['bp'], na, flipud, r['gamma'])
+        out = [_out(Tx, astensor, is2), _out(W3, astensor, is2), fp['f_asc'][::-1],
+               _scales_out(r, astensor)]
+        if get_w:
+            out.append(_out(r['w'], astensor, is2))
+        if get_dWx:
+            out.append(_out(r['dWx'], astensor, is2))
+        return tuple(out)
     fp = _ssq_plan(wavelet, scales, N, nv, ssq_freqs, maprange, padtype, dt, sp)
     f_asc = fp['f_asc']
     def run(xin):
@@ -477,7 +534,7 @@ def ssq_cwt(x, wavelet='gmw', scales='log-piecewise', nv=None, fs=None, t=None,
 
 def _ssq_cwt_by_differences(x, wavelet, kernel, scales, nv, fs, t, dt, padtype,
                             nan_checks, gamma, sp, ssq_freqs, maprange, flipud,
-                            difftype, difforder, astensor, get_dWx):
+                            difftype, difforder, astensor, get_dWx, squeezing='sum'):
     """`ssq_cwt` with difftype 'phase' or 'numeric' (get_w=True): the phase
     transform from differences of Wx along time (`ssqb_phase_diff`), then the
     squeeze from it (`ssqb_indexed_sum`). 'numeric' works on the padded
@@ -506,17 +563,14 @@ def _ssq_cwt_by_differences(x, wavelet, kernel, scales, nv, fs, t, dt, padtype,
                                  float(r['gamma']), prec, L.ptr(w), L.stream_ptr())
         L.check(rc, 'phase_diff')
         Ws = W[..., col0:col0 + M].contiguous() if numeric else W
-        Tx = torch.empty_like(Ws)
-        cst = _on_device(fp, 'const', dev)
-        cb = L.make_bins(fp['mode'], fp['bp'], na, flipud)
-        rc = lib.ssqb_indexed_sum(L.ptr(Ws), L.ptr(w), L.ptr(cst), cb, B, na, M, prec,
-                                  L.ptr(Tx), L.stream_ptr())
-    L.check(rc, 'squeeze')
+    is2 = r['is_2d']
+    Wv = _squeeze_values(Ws if is2 else Ws[0], squeezing)
+    Tx = _squeeze_from(Wv if is2 else Wv[None], w, None, None,
+                       _on_device(fp, 'const', dev), fp['mode'], fp['bp'], na, flipud, 0.)
     if numeric:
         # Tx and w lose the 4 extra columns each side; the returned Wx is the
         # padded transform less 4 columns each side (_ssq_cwt.py:294-296)
         Ws, Tx, w = (a[..., 4:-4].contiguous() for a in (W, Tx, w))
-    is2 = r['is_2d']
     out = [_out(Tx, astensor, is2), _out(Ws, astensor, is2), fp['f_asc'][::-1],
            _scales_out(r, astensor), _out(w, astensor, is2)]
     if get_dWx:
@@ -734,21 +788,15 @@ def ssqueeze(Wx, w=None, ssq_freqs=None, scales=None, Sfs=None, fs=None, t=None,
         const = P.squeeze_weights(None, None, None, 'stft', ssq_freqs=f)
         sfs = _dev_f64(P._to_numpy(Sfs), dev) if Sfs is not None else None
     mode, bp = P.bin_params(f, logscale)
-    cb = L.make_bins(mode, bp, na, flipud)
-    prec = L.F64 if W3.dtype == torch.complex128 else L.F32
-    Tx = torch.empty_like(W3)
     cst = _dev_f64(const, dev)
-    with torch.cuda.device(dev):
-        if w is not None:
-            rc = L.load().ssqb_indexed_sum(L.ptr(W3), L.ptr(wt), L.ptr(cst), cb,
-                                           B, na, N, prec, L.ptr(Tx),
-                                           L.stream_ptr())
-        else:
-            dW = torch.as_tensor(dWx).to(dev).contiguous()
-            rc = L.load().ssqb_ssqueeze_fast(L.ptr(W3), L.ptr(dW), L.ptr(sfs),
-                                             L.ptr(cst), cb, float(gamma), B, na,
-                                             N, prec, L.ptr(Tx), L.stream_ptr())
-    L.check(rc, 'ssqueeze')
+    Wv = _squeeze_values(W, squeezing)
+    Wv = Wv if W.ndim == 3 else Wv[None]
+    dW = None
+    if w is None:
+        dW = torch.as_tensor(dWx).to(dev).contiguous()
+        dW = dW if dW.ndim == 3 else dW[None]
+    Tx = _squeeze_from(Wv, wt if w is not None else None, dW, sfs, cst, mode, bp, na,
+                       flipud, gamma if gamma is not None else 0.)
     Tx = Tx if W.ndim == 3 else Tx[0]
     if (transform == 'cwt' and not flipud) or flipud:
         f = f[::-1]
@@ -1005,7 +1053,20 @@ def ssq_stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=Non
     mode, bp = P.bin_params(f, False)
     const = P.squeeze_weights(None, None, None, 'stft', ssq_freqs=f)
 
+    plain = isinstance(squeezing, str) and squeezing == 'sum'
+
     def run(xin):
+        if not plain:
+            # the squeeze sums other values than Sx (ssqueezing.py:196-201)
+            r = _stft_core(xin, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
+                           True, dtype, want_w=get_w, gamma=gamma, flipud=flipud)
+            is2 = r['is_2d']
+            Sv = _squeeze_values(r['Sx'] if is2 else r['Sx'][0], squeezing)
+            cst = _dev_f64(const, r['dev'])
+            Tx = _squeeze_from(Sv if is2 else Sv[None], r['w'], r['dSx'],
+                               _dev_f64(r['Sfs'], r['dev']), cst, mode, bp, r['nrow'],
+                               flipud, r['gamma'])
+            return Tx, r, cst
         r = _stft_core(xin, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
                        get_dWx, dtype, want_idx=True, want_w=get_w, bins=(mode, bp),
                        gamma=gamma, flipud=flipud)
@@ -1021,6 +1082,8 @@ def ssq_stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=Non
 
     if A.needs_grad(x):
         _grad_checks(astensor, False, padtype)
+        if not plain:
+            raise NotImplementedError("gradients need squeezing='sum'")
         holder = {}
 
         def run_keep(xin):

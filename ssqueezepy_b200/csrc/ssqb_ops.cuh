@@ -194,6 +194,17 @@ __device__ __forceinline__ int bin_of_fast(const BinDev& bp, float w) {
 // The bin is decided in float32 when that is safe, else in float64; either
 // way it equals the float64 decision from these values. Returns kNoBin where
 // |Wx| <= gamma.
+// The phase transform alone (inf where |Wx| < gamma), for outputs that ask
+// for w without a bin index.
+template <typename C>
+__device__ __forceinline__ double phase_w(C Wv, C dWv, double sfs, bool stft, double gamma) {
+  const double c = Wv.x, d = Wv.y, a = dWv.x, b = dWv.y;
+  const double m2 = c * c + d * d;
+  const double ph = (b * c - a * d) / (m2 * kTwoPi);
+  const double wv = stft ? fabs(sfs - ph) : fabs(ph);
+  return (m2 < gamma * gamma) ? __longlong_as_double(0x7ff0000000000000ULL) : wv;
+}
+
 template <typename C>
 __device__ __forceinline__ uint16_t phase_bin(C Wv, C dWv, double sfs, bool stft,
                                               const BinDev& bp, double gamma,
@@ -202,11 +213,7 @@ __device__ __forceinline__ uint16_t phase_bin(C Wv, C dWv, double sfs, bool stft
   const double m2 = c * c + d * d;
   const double num = b * c - a * d;
   const bool keep = m2 > gamma * gamma;  // |Wx| > gamma
-  if (w_out) {
-    const double ph = num / (m2 * kTwoPi);
-    const double wv = stft ? fabs(sfs - ph) : fabs(ph);
-    *w_out = (m2 < gamma * gamma) ? __longlong_as_double(0x7ff0000000000000ULL) : wv;
-  }
+  if (w_out) *w_out = phase_w(Wv, dWv, sfs, stft, gamma);
   if (!keep) return kNoBin;
   int k = -2;
   {
@@ -349,13 +356,15 @@ struct CwtOp {
     const size_t o = ((size_t)b * na + row) * N + j;
     if (Wx) Wx[o] = out_c<OC>(Wv);
     if (dWx) dWx[o] = out_c<OC>(dWv);
-    if (idx || w) {
+    if (idx) {
       // bins from the arithmetic-precision values, before output rounding
       double wv;
       const uint16_t k = phase_bin(Wv, dWv, 0.0, false, bins, gamma, status,
                                    w ? &wv : nullptr);
-      if (idx) idx[((size_t)b * na + row) * idx_pitch + j] = k;
+      idx[((size_t)b * na + row) * idx_pitch + j] = k;
       if (w) w[o] = (OT)wv;
+    } else if (w) {
+      w[o] = (OT)phase_w(Wv, dWv, 0.0, false, gamma);  // no bins asked for
     }
   }
 };
@@ -404,12 +413,14 @@ struct StftOp {
     const size_t o = ((size_t)b * nrow + n) * nframes + t;
     if (Sx) Sx[o] = out_c<OC>(S);
     if (dSx) dSx[o] = out_c<OC>(dS);
-    if (idx || w) {
+    if (idx) {
       double wv;
       const uint16_t k = phase_bin(S, dS, __ldg(sfs + n), true, bins, gamma, status,
                                    w ? &wv : nullptr);
-      if (idx) idx[((size_t)b * nrow + n) * idx_pitch + t] = k;
+      idx[((size_t)b * nrow + n) * idx_pitch + t] = k;
       if (w) w[o] = (OT)wv;
+    } else if (w) {
+      w[o] = (OT)phase_w(S, dS, __ldg(sfs + n), true, gamma);  // no bins asked for
     }
   }
 };

@@ -34,8 +34,15 @@ Writes:
                    1, 2, 4), get_w=True, float64, and phase_cwt /
                    phase_cwt_num of the same Wx
 
+  squeezing.npz    ssq_cwt / ssq_stft with squeezing 'lebesgue', 'abs' and a
+                   function (W * W), with and without get_w, float64
+
+  utils.npz        padsignal (five modes, default and given lengths) and
+                   get_window (with derivative) outputs
+
 `--only issq` / `--only ridges` / `--only higher` / `--only istft` /
-`--only difftype` writes that file alone.
+`--only difftype` / `--only squeezing` / `--only utils` writes that file
+alone.
 """
 import os
 import sys
@@ -346,6 +353,53 @@ def difftype_fixtures(ref_root):
     np.savez_compressed(os.path.join(HERE, 'difftype.npz'), **out)
 
 
+def square(W):
+    """A squeezing function that works on numpy arrays and torch tensors."""
+    return W * W
+
+
+def squeezing_fixtures(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    from ssqueezepy import Wavelet
+    x = chirp_signal(256, seed=8)
+    out = dict(x=x)
+    w = Wavelet(('gmw', dict(dtype='float64')))
+    for name, sqz in (('lebesgue', 'lebesgue'), ('abs', 'abs'), ('square', square)):
+        Tx, *_ = sq.ssq_cwt(x, w, nv=8, squeezing=sqz, astensor=False)
+        out['cwt_%s/Tx' % name] = Tx
+        Tx, *_ = sq.ssq_cwt(x, w, nv=8, squeezing=sqz, get_w=True, astensor=False)
+        out['cwt_%s_w/Tx' % name] = Tx
+        Tx, *_ = sq.ssq_stft(x, 'hann', n_fft=64, squeezing=sqz, dtype='float64',
+                             astensor=False)
+        out['stft_%s/Tx' % name] = Tx
+    np.savez_compressed(os.path.join(HERE, 'squeezing.npz'), **out)
+
+
+PAD_CASES = [(pt, pl) for pt in ('zero', 'reflect', 'symmetric', 'replicate', 'wrap')
+             for pl in (None, 64, 77)]
+WINDOW_CASES = [('hann', 64, None), ('hamming', 48, 64), (None, 64, None)]
+
+
+def utils_fixtures(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    from ssqueezepy.utils import padsignal
+    x = np.random.default_rng(21).standard_normal((3, 37))
+    out = dict(x=x)
+    for pt, pl in PAD_CASES:
+        xp, n_up, n1, n2 = padsignal(x, pt, pl, get_params=True)
+        out['pad_%s_%s' % (pt, pl)] = xp
+        out['pad_%s_%s_geom' % (pt, pl)] = np.array([n_up, n1, n2])
+    for win, wl, nf in WINDOW_CASES:
+        w, dw = sq.get_window(win, wl, nf, derivative=True)
+        out['win_%s_%d_%s' % (win, wl, nf)] = w
+        out['dwin_%s_%d_%s' % (win, wl, nf)] = dw
+    np.savez_compressed(os.path.join(HERE, 'utils.npz'), **out)
+
+
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
     root = args[0] if args else '/root/reference'
@@ -359,6 +413,10 @@ if __name__ == '__main__':
         istft_fixtures(root)
     elif '--only' in sys.argv and 'difftype' in sys.argv:
         difftype_fixtures(root)
+    elif '--only' in sys.argv and 'squeezing' in sys.argv:
+        squeezing_fixtures(root)
+    elif '--only' in sys.argv and 'utils' in sys.argv:
+        utils_fixtures(root)
     else:
         main(root)
         issq_fixtures(root)
@@ -366,3 +424,5 @@ if __name__ == '__main__':
         higher_fixtures(root)
         istft_fixtures(root)
         difftype_fixtures(root)
+        squeezing_fixtures(root)
+        utils_fixtures(root)
