@@ -334,6 +334,21 @@ SSQB_API int ssqb_phase_diff(const void* Wx, int B, int na, int ncol, int col0, 
                              int mode, int difforder, double dt, double gamma,
                              int precision, void* w, void* stream);
 
+/* Workspace bytes of ssqb_trigdiff: the spectra of a chunk of rows (up to
+ * 256 MB of them, at least one row) and the two-pass intermediate. */
+SSQB_API size_t ssqb_trigdiff_workspace_bytes(int rows, int Npad);
+
+/* Frequency-domain derivative of rows (trigdiff, utils/common.py:161-245):
+ * D = ifft(fft(Ap) * i xi fs), xi_k = 2 pi kk / Npad with kk = k for
+ * k <= Npad/2 and k - Npad above (no Nyquist halving), Ap = A padded to Npad
+ * with n1 samples on the left by padtype (5 = none: A is already Npad long,
+ * n1 = 0). out (rows, N_out) = D[:, out_off : out_off + N_out]. A and out
+ * complex of the data precision; float64 arithmetic. Npad a power of two in
+ * [8, 2^22]. */
+SSQB_API int ssqb_trigdiff(const void* A, int rows, int M, int Npad, int n1, int padtype,
+                           double fs, int out_off, int N_out, int precision, void* out,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
 /* Workspace bytes of ssqb_istft: the real frames, B * n_fft * n_frames
  * elements of the data precision. */
 SSQB_API size_t ssqb_istft_workspace_bytes(int B, int n_fft, int n_frames, int precision);

@@ -70,6 +70,8 @@ SIGNATURES = {
     'ssqb_stft_adjoint': (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _i,
                                _vp, _i, _vp, _sz, _vp]),
     'ssqb_phase_diff': (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _d, _d, _i, _vp, _vp]),
+    'ssqb_trigdiff_workspace_bytes': (_sz, [_i, _i]),
+    'ssqb_trigdiff': (_i, [_vp, _i, _i, _i, _i, _i, _d, _i, _i, _i, _vp, _vp, _sz, _vp]),
     'ssqb_istft_workspace_bytes': (_sz, [_i, _i, _i, _i]),
     'ssqb_istft': (_i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _d, _i, _vp, _vp, _sz, _vp]),
     'ssqb_squeeze_adjoint': (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _i, _vp]),

@@ -955,6 +955,68 @@ def stft(x, window=None, n_fft=None, win_len=None, hop_len=1, fs=None, t=None,
     return (Sx, dSx) if derivative else Sx
 
 
+def trigdiff(A, fs=1., padtype=None, rpadded=None, N=None, n1=None, window=None,
+             transform='cwt'):
+    """Frequency-domain derivative of the rows of `A` (trigdiff,
+    utils/common.py:161-245): ifft(fft(A) * 1j * xi * fs) along the last axis,
+    A padded first unless `rpadded` (padtype defaults to 'reflect' then), and
+    the result cut to columns n1 .. n1 + N of the padded length (N defaults to
+    the padded length and the cut stops at its end, as in the reference).
+    On the GPU (`ssqb_trigdiff`); numpy in, numpy out."""
+    if transform == 'stft':
+        raise NotImplementedError("`transform='stft'` is currently not supported.")
+    is_np = isinstance(A, np.ndarray)
+    T = torch.as_tensor(A)
+    if T.ndim not in (2, 3):
+        raise AssertionError("`A` must be 2D or 3D (got %s dims)" % T.ndim)
+    if rpadded and N is None:
+        raise ValueError("must pass `N` if `rpadded`")
+    rpadded = rpadded or False
+    padtype = padtype or ('reflect' if not rpadded else None)
+    M = T.shape[-1]
+    if padtype is not None:
+        # padsignal (utils/common.py:54-158): 1D / 2D only; tensors 'zero' or
+        # 'reflect', numpy arrays all five modes
+        supported = ('zero', 'reflect', 'symmetric', 'replicate', 'wrap') if is_np else \
+            ('zero', 'reflect')
+        if padtype not in supported:
+            raise ValueError("`padtype` must be one of: %s (got %s)"
+                             % (', '.join(supported), padtype))
+        if T.ndim != 2:
+            raise ValueError("`x` must be 1D or 2D (got x.ndim == %s)" % T.ndim)
+        Npad, n1, _ = P.p2up(M)  # the padding's n1 replaces the argument's
+        ptype = L.PADTYPES[padtype]
+    else:
+        Npad, ptype = M, 5
+        if Npad & (Npad - 1) or Npad < 8 or Npad > (1 << 22):
+            raise NotImplementedError("trigdiff of an unpadded length needs a power of "
+                                      "two in [8, 2^22] on the accelerated path")
+        if n1 is None:
+            _, n1, _ = P.p2up(N)
+    Nn = N if N is not None else Npad
+    N_out = min(Nn, Npad - n1)
+    if N_out < 1:
+        raise ValueError("empty output: n1=%s, N=%s, padded length %s" % (n1, Nn, Npad))
+    L.require_cuda()
+    dev = _device_of(A)
+    cdt = torch.complex128 if T.dtype in (torch.complex128, torch.float64) else \
+        torch.complex64
+    T = T.to(device=dev, dtype=cdt).contiguous()
+    rows = T.numel() // M
+    out = torch.empty(T.shape[:-1] + (N_out,), dtype=cdt, device=dev)
+    lib = L.load()
+    wsb = lib.ssqb_trigdiff_workspace_bytes(rows, Npad)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    prec = L.F64 if cdt == torch.complex128 else L.F32
+    with torch.cuda.device(dev):
+        pad_n1 = n1 if padtype is not None else 0   # left pad of the input
+        rc = lib.ssqb_trigdiff(L.ptr(T), rows, M, Npad, int(pad_n1), ptype, float(fs),
+                               int(n1), int(N_out), prec, L.ptr(out), L.ptr(ws), wsb,
+                               L.stream_ptr())
+    L.check(rc, 'trigdiff')
+    return out.cpu().numpy() if is_np else out
+
+
 def _istft_plan(window, win_len, n_fft, hop_len, win_exp, dtype):
     """Window powers of the inverse STFT and the NOLA checks' warnings
     (_stft.py:230-237, 313-337), cached. The window is rounded to the data

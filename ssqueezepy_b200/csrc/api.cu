@@ -811,6 +811,54 @@ int ssqb_phase_diff(const void* Wx, int B, int na, int ncol, int col0, int M, in
   return SSQB_OK;
 }
 
+static size_t trigdiff_chunk(int rows, int Npad) {
+  const size_t per = (size_t)Npad * sizeof(double2);
+  size_t c = ((size_t)256 << 20) / per;
+  if (c < 1) c = 1;
+  return c < (size_t)rows ? c : (size_t)rows;
+}
+
+size_t ssqb_trigdiff_workspace_bytes(int rows, int Npad) {
+  if (rows < 1 || !is_pow2(Npad)) return 0;
+  const size_t z = kZBudgetBytes > (size_t)Npad * sizeof(double2)
+                       ? kZBudgetBytes : (size_t)Npad * sizeof(double2);
+  return trigdiff_chunk(rows, Npad) * Npad * sizeof(double2) + z;
+}
+
+int ssqb_trigdiff(const void* A, int rows, int M, int Npad, int n1, int padtype, double fs,
+                  int out_off, int N_out, int precision, void* out, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+  if (!A || !out || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (rows < 1 || M < 1 || N_out < 1) return fail(SSQB_EINVAL, "rows, M, N_out must be >= 1");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
+    return fail(SSQB_EUNSUPPORTED, "Npad must be a power of two in [8, 2^22]");
+  if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
+  if (n1 < 0 || (long long)n1 + M > Npad) return fail(SSQB_EINVAL, "bad padding geometry");
+  if (padtype == 5 && (n1 != 0 || M != Npad))
+    return fail(SSQB_EINVAL, "padtype 5 (none) needs M == Npad and n1 == 0");
+  if (out_off < 0 || (long long)out_off + N_out > Npad)
+    return fail(SSQB_EINVAL, "output columns must lie in [0, Npad)");
+  const size_t need = ssqb_trigdiff_workspace_bytes(rows, Npad);
+  if (workspace_bytes < need)
+    return fail(SSQB_EWORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                     " bytes");
+  Tables tb;
+  int r = get_tables(&tb);
+  if (r) return r;
+  const int chunk = (int)trigdiff_chunk(rows, Npad);
+  double2* xh = (double2*)workspace;
+  double2* Z = xh + (size_t)chunk * Npad;
+  const size_t zcap = (workspace_bytes - (size_t)chunk * Npad * sizeof(double2)) /
+                      sizeof(double2);
+  const int e = run_trigdiff(A, data_prec(precision) == SSQB_F64, rows, M, Npad, n1, padtype,
+                             fs, out_off, N_out, out, xh, chunk, Z, zcap, tb,
+                             (cudaStream_t)stream);
+  if (e) return cuda_fail((cudaError_t)e, "trigdiff launch");
+  return SSQB_OK;
+}
+
 size_t ssqb_istft_workspace_bytes(int B, int n_fft, int n_frames, int precision) {
   if (B < 1 || n_frames < 1 || !is_pow2(n_fft) || !valid_precision(precision)) return 0;
   const size_t rs = data_prec(precision) == SSQB_F64 ? sizeof(double) : sizeof(float);

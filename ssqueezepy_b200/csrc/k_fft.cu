@@ -62,6 +62,37 @@ int run_cwt_f32x(const CwtOp<double2, float2>& op, int B, int log2L, double2* Z,
                                                                tb, st);
 }
 
+// trigdiff: rows in chunks of `chunk` through the spectrum buffer xh
+template <typename TC, typename OC>
+static int run_trigdiff_t(const TC* A, int rows, int M, int Npad, int n1, int padtype,
+                          double fs, int out_off, int N_out, OC* out, double2* xh, int chunk,
+                          double2* Z, size_t zcap, const Tables& tb, cudaStream_t st) {
+  const int m = ilog2(Npad);
+  for (int r0 = 0; r0 < rows; r0 += chunk) {
+    const int nr = (rows - r0) < chunk ? (rows - r0) : chunk;
+    RowFftOp<TC> f{A, xh, M, Npad, n1, padtype, r0, nr};
+    int e = run_tile<RowFftOp<TC>, double2, -1>(f, 1, nr, m, Z, zcap, tb, st);
+    if (e) return e;
+    RowDiffOp<OC> d{xh, out, Npad, r0, nr, out_off, N_out, 2.0 * M_PI / Npad * fs,
+                    1.0 / Npad};
+    e = run_tile<RowDiffOp<OC>, double2, 1>(d, 1, nr, m, Z, zcap, tb, st);
+    if (e) return e;
+  }
+  return 0;
+}
+
+int run_trigdiff(const void* A, bool f64, int rows, int M, int Npad, int n1, int padtype,
+                 double fs, int out_off, int N_out, void* out, double2* xh, int chunk,
+                 double2* Z, size_t zcap, const Tables& tb, cudaStream_t st) {
+  if (f64)
+    return run_trigdiff_t<double2, double2>((const double2*)A, rows, M, Npad, n1, padtype, fs,
+                                            out_off, N_out, (double2*)out, xh, chunk, Z, zcap,
+                                            tb, st);
+  return run_trigdiff_t<float2, float2>((const float2*)A, rows, M, Npad, n1, padtype, fs,
+                                        out_off, N_out, (float2*)out, xh, chunk, Z, zcap, tb,
+                                        st);
+}
+
 int run_xhat_batch_f32(const float* x, const SigDesc* desc, int nsig, int Npad, int padtype,
                        double2* xh, double2* Z, size_t zcap, const Tables& tb,
                        cudaStream_t st) {

@@ -100,6 +100,9 @@ void set_launch_counter(int* c);
 int* launch_counter();
 
 // batches of uneven lengths sharing one padded length (float32 data)
+int run_trigdiff(const void* A, bool f64, int rows, int M, int Npad, int n1, int padtype,
+                 double fs, int out_off, int N_out, void* out, double2* xh, int chunk,
+                 double2* Z, size_t zcap, const Tables& tb, cudaStream_t st);
 int run_xhat_batch_f32(const float* x, const SigDesc* desc, int nsig, int Npad, int padtype,
                        double2* xh, double2* Z, size_t zcap, const Tables& tb,
                        cudaStream_t st);

@@ -271,6 +271,63 @@ template <> __device__ __forceinline__ double2 out_c<double2>(double2 v) { retur
 template <typename OC> __device__ __forceinline__ OC out_c(float2 v);
 template <> __device__ __forceinline__ float2 out_c<float2>(float2 v) { return v; }
 
+// ---- trigdiff (utils/common.py:161-245): D = ifft(fft(pad(A)) * i xi fs) ------
+// Rows of a complex array as the rows of one batch item: the forward
+// transform of each padded row into a spectrum buffer, then the derivative
+// factor and the inverse transform, stored from column out_off on. Rows
+// row0 .. row0 + nrows - 1 of A per call (the spectrum buffer holds nrows).
+template <typename TC>
+struct RowFftOp {
+  static constexpr int NARR = 1;
+  static constexpr bool kDirect = true;
+  static constexpr bool kBatch = false;
+  const TC* A;      // (rows, M)
+  double2* xh;      // (nrows, Npad)
+  int M, Npad, n1, padtype, row0, nrows;
+  __device__ RowFftOp bind(int) const { return *this; }
+  __device__ int rows() const { return nrows; }
+  __device__ void load(int, int row, int k, double2 (&v)[1]) const {
+    const int s = pad_src((long long)k - n1, M, padtype);
+    if (s >= 0) {
+      const TC a = A[(size_t)(row0 + row) * M + s];
+      v[0] = make_double2((double)a.x, (double)a.y);
+    } else {
+      v[0] = make_double2(0.0, 0.0);
+    }
+  }
+  __device__ void store(int, int row, int n, double2 (&v)[1]) const {
+    xh[(size_t)row * Npad + n] = v[0];
+  }
+};
+
+template <typename OC>
+struct RowDiffOp {
+  static constexpr int NARR = 1;
+  static constexpr bool kDirect = true;
+  static constexpr bool kBatch = false;
+  const double2* xh;  // (nrows, Npad)
+  OC* out;            // (rows, N_out)
+  int Npad, row0, nrows, out_off, N_out;
+  double h_fs;        // 2 pi / Npad * fs
+  double inv_npad;
+  __device__ RowDiffOp bind(int) const { return *this; }
+  __device__ int rows() const { return nrows; }
+  __device__ void load(int, int row, int k, double2 (&v)[1]) const {
+    // xi_k = k h (k <= Npad/2), (k - Npad) h otherwise (wavelets.py:473-484,
+    // no Nyquist halving here)
+    const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
+    const double c = (double)kk * h_fs;
+    const double2 z = xh[(size_t)row * Npad + k];
+    v[0] = make_double2(-z.y * c, z.x * c);
+  }
+  __device__ void store(int, int row, int n, double2 (&v)[1]) const {
+    const int j = n - out_off;
+    if (j < 0 || j >= N_out) return;
+    out[(size_t)(row0 + row) * N_out + j] =
+        out_c<OC>(make_double2(v[0].x * inv_npad, v[0].y * inv_npad));
+  }
+};
+
 template <typename C, typename OC = C>
 struct CwtOp {
   typedef typename RealOf<C>::type T;

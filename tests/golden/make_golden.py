@@ -38,7 +38,9 @@ Writes:
                    function (W * W), with and without get_w, float64
 
   utils.npz        padsignal (five modes, default and given lengths) and
-                   get_window (with derivative) outputs
+                   get_window (with derivative) outputs; trigdiff of seeded
+                   complex rows (default reflect padding without N, zero
+                   padding with N, already padded 2D and 3D input)
 
 `--only issq` / `--only ridges` / `--only higher` / `--only istft` /
 `--only difftype` / `--only squeezing` / `--only utils` writes that file
@@ -397,6 +399,15 @@ def utils_fixtures(ref_root):
         w, dw = sq.get_window(win, wl, nf, derivative=True)
         out['win_%s_%d_%s' % (win, wl, nf)] = w
         out['dwin_%s_%d_%s' % (win, wl, nf)] = dw
+    from ssqueezepy.utils import trigdiff
+    rng = np.random.default_rng(22)
+    A = rng.standard_normal((5, 300)) + 1j * rng.standard_normal((5, 300))
+    Ap = rng.standard_normal((2, 3, 512)) + 1j * rng.standard_normal((2, 3, 512))
+    out['td_A'], out['td_Ap'] = A, Ap
+    out['td_reflect'] = trigdiff(A, fs=2.)
+    out['td_zero_N'] = trigdiff(A, fs=1., padtype='zero', N=300)
+    out['td_rpadded'] = trigdiff(Ap[0], fs=3., rpadded=True, N=300)
+    out['td_rpadded3'] = trigdiff(Ap, rpadded=True, N=256, n1=100)
     np.savez_compressed(os.path.join(HERE, 'utils.npz'), **out)
 
 
