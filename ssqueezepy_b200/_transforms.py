@@ -148,8 +148,10 @@ def _scales_plan(scales, N, wavelet, nv):
         else:
             sc, st, na, nv_ = P.process_scales(P._to_numpy(scales), N,
                                                get_params=True)
+        # `scales_in` keeps the caller's dtype: inferring the scale type of
+        # float32 scales takes float32 tolerances (cwt_utils.py:375-394)
         return dict(scales=np.asarray(sc, np.float64).ravel(), scaletype=st,
-                    na=na, nv=nv_)
+                    na=na, nv=nv_, scales_in=np.asarray(sc).reshape(-1, 1))
     return _plan(('scales', _wkey(wavelet), N, _akey(scales), nv), make)
 
 
@@ -423,12 +425,12 @@ def _ssq_plan(wavelet, scales, N, nv, ssq_freqs, maprange, padtype, dt, sp=None)
 
     def make():
         f_asc, logscale = _ssq_freqs_for_cwt(
-            ssq_freqs, sc.reshape(-1, 1), N, wavelet, cwt_st, maprange,
+            ssq_freqs, sp['scales_in'], N, wavelet, cwt_st, maprange,
             padtype is not None, dt)
         mode, bp = P.bin_params(f_asc, logscale)
         # ssqueeze re-derives (scaletype, nv) from the scale array, so a
         # log-piecewise grid gets ln2/nv per row (ssqueezing.py:168-169, 124-128)
-        _, st_a, _, nv_a = P.process_scales(sc.reshape(-1, 1), N, get_params=True)
+        _, st_a, _, nv_a = P.process_scales(sp['scales_in'], N, get_params=True)
         const = P.squeeze_weights(sc, st_a, nv_a, 'cwt')
         return dict(f_asc=f_asc, mode=mode, bp=bp, const=const)
     return _plan(('ssq', _wkey(wavelet), N, _akey(scales), nv, _akey(ssq_freqs),
@@ -642,17 +644,23 @@ def _icwt_plan(wavelet, scales, x_len, nv, l1_norm):
         else:
             sc, st, _, nv_ = P.process_scales(P._to_numpy(scales), x_len,
                                               get_params=True)
+        # the transition of log-piecewise scales is found at the caller's
+        # dtype (float32 tolerances for float32 scales, cwt_utils.py:385)
+        idx = (P.logscale_transition_idx(np.asarray(sc).ravel())
+               if st == 'log-piecewise' else None)
         sc = np.asarray(sc, np.float64).ravel()
-        weights, mean_mult = _icwt_weights(sc, st, P.adm_ssq(wavelet), l1_norm)
+        weights, mean_mult = _icwt_weights(sc, st, P.adm_ssq(wavelet), l1_norm, idx)
         return dict(weights=weights, mean_mult=mean_mult)
     return _plan(('icwt', _wkey(wavelet), x_len, _akey(scales), nv, l1_norm), make)
 
 
-def _icwt_weights(scales, scaletype, Cpsi, l1_norm):
+def _icwt_weights(scales, scaletype, Cpsi, l1_norm, idx=None):
     """Per-row weights and the x_mean multiplicity of the one-integral inverse
-    (_cwt.py:422-452, 479-494)."""
+    (_cwt.py:422-452, 479-494); `idx` the log-piecewise transition when known."""
     if scaletype == 'log-piecewise':
-        idx = P.logscale_transition_idx(scales)
+        idx = P.logscale_transition_idx(scales) if idx is None else idx
+        if idx is None:
+            raise ValueError("log-piecewise scales without a transition index")
         w0, _ = _icwt_weights(scales[:idx], 'log', Cpsi, l1_norm)
         w1, _ = _icwt_weights(scales[idx:], 'log', Cpsi, l1_norm)
         return np.concatenate([w0, w1]), 2.0  # each piece adds x_mean

@@ -108,3 +108,23 @@ def test_ssq_plan_weights_follow_scale_array():
     idx = P.logscale_transition_idx(s)
     assert idx is not None
     assert np.allclose(c[:idx], np.log(2) / 32) and np.allclose(c[idx:], np.log(2) / 8)
+
+
+def test_float32_scale_arrays_plan_like_float64():
+    """Scales handed back at float32 (as ssq_cwt returns them for float32
+    data) keep their log-piecewise type: the transition is found at float32
+    tolerances, as the reference does (cwt_utils.py:375-394), for the squeeze
+    bins and weights and for icwt's pieces."""
+    import numpy as np
+    from ssqueezepy_b200 import _params as P
+    from ssqueezepy_b200 import _transforms as T
+    w = P.Wavelet('gmw', N=1024)
+    sc64 = P.process_scales('log-piecewise', 1024, w, nv=32).ravel()
+    out = []
+    for sc in (sc64, sc64.astype(np.float32)):
+        sp = T._scales_plan(sc, 1024, w, None)
+        fp = T._ssq_plan(w, sc, 1024, None, None, 'peak', 'reflect', 1.0, sp)
+        ip = T._icwt_plan(w, sc, 1024, None, True)
+        out.append((sp['scaletype'], fp['mode'], fp['bp'][4], len(ip['weights']),
+                    ip['mean_mult']))
+    assert out[0] == out[1] == ('log-piecewise', 1, out[0][2], len(sc64), 2.0)
