@@ -23,8 +23,13 @@ def extract_ridges(Tf, scales, penalty=2., n_ridges=1, bw=15, transform='cwt',
                    get_params=False, parallel=True):
     is_np = isinstance(Tf, np.ndarray)
     T = torch.as_tensor(Tf)
-    if not T.is_complex() or T.ndim != 2:
-        raise ValueError("`Tf` must be a 2D complex array (frequencies, time)")
+    if T.ndim != 2:
+        raise ValueError("`Tf` must be a 2D array (frequencies, time)")
+    if not T.is_complex():
+        # real (or integer) input: the reference takes float32 eps, scales and
+        # penalty for anything but complex128 (ridge_extraction.py:113-115);
+        # here its energies are float32 too
+        T = T.to(torch.complex64)
     if transform not in ('cwt', 'stft'):
         raise ValueError("`transform` must be 'cwt' or 'stft' (got %s)" % transform)
     L.require_cuda()
