@@ -150,7 +150,9 @@ SSQB_API int ssqb_indexed_sum(const void* Wx, const void* w, const double* row_w
  * (n_fft) double, diff_window already scaled as the reference does (times
  * fs when modulated); Sfs (n_fft/2+1) double. Outputs (B, n_fft/2+1,
  * n_frames), n_frames = (N-1)/hop + 1; dSx, w, idx optional. n_fft is a
- * power of two <= 4096; n1 is the left pad of the N + n_fft - 1 padding. */
+ * power of two <= 4096, or any length in [4, 1024] (Bluestein's chirp-z
+ * transform through a power-of-two length >= 2 n_fft - 1, float64
+ * arithmetic); n1 is the left pad of the N + n_fft - 1 padding. */
 SSQB_API int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padtype,
               int modulated, const double* window, const double* diff_window,
               const double* Sfs, const ssqb_bins* bins, double gamma, int precision,

@@ -899,9 +899,11 @@ def _stft_core(x, window, n_fft, win_len, hop_len, fs, t, padtype, modulated,
                    else n_fft)
     dtype = P._dtype_str(dtype or P.DEFAULTS['stft_dtype'])
     win, dwin = P.get_window(window, win_len, n_fft, derivative=True)
-    if n_fft & (n_fft - 1) or n_fft < 8 or n_fft > 4096:
-        raise NotImplementedError("n_fft must be a power of two in [8, 4096] on "
-                                  "the accelerated path (got %s)" % n_fft)
+    if (n_fft & (n_fft - 1) == 0 and not 8 <= n_fft <= 4096) or \
+            (n_fft & (n_fft - 1) and not 4 <= n_fft <= 1024):
+        raise NotImplementedError("n_fft must be a power of two in [8, 4096] or any "
+                                  "length in [4, 1024] on the accelerated path "
+                                  "(got %s)" % n_fft)
     if len(win) != n_fft:
         raise ValueError("window length %s != n_fft %s" % (len(win), n_fft))
     if padtype not in L.PADTYPES:

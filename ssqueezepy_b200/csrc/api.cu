@@ -412,12 +412,20 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
     return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || hop < 1) return fail(SSQB_EINVAL, "B, N and hop must be >= 1");
   if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
-  if (!is_pow2(n_fft) || n_fft < 8 || n_fft > 4096)
-    return fail(SSQB_EUNSUPPORTED, "n_fft must be a power of two in [8, 4096]");
+  const bool pow2 = is_pow2(n_fft);
+  // other lengths go through Bluestein's transform of length M >= 2 n_fft - 1,
+  // which must fit one float64 tile
+  int log2M = 0;
+  while ((1 << log2M) < 2 * n_fft - 1) ++log2M;
+  if (pow2 ? (n_fft < 8 || n_fft > 4096)
+           : (n_fft < 4 || (1 << log2M) > FftCfg<double2>::TILE))
+    return fail(SSQB_EUNSUPPORTED,
+                "n_fft must be a power of two in [8, 4096] or any length in [4, " +
+                    std::to_string((FftCfg<double2>::TILE + 1) / 2) + "]");
   if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");
   if (!valid_precision(precision))
     return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
-  if (precision != SSQB_F32 && n_fft > FftCfg<double2>::TILE)
+  if (pow2 && precision != SSQB_F32 && n_fft > FftCfg<double2>::TILE)
     return fail(SSQB_EUNSUPPORTED, "n_fft above " + std::to_string(FftCfg<double2>::TILE) +
                                        " needs float32 arithmetic");
   const int nrow = n_fft / 2 + 1;
@@ -437,7 +445,21 @@ int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, int padty
   const int s21 = (n_fft % 2 == 1) ? s20 - 1 : s20;
   const int m = ilog2i(n_fft);
   int e;
-  if (precision == SSQB_F32) {
+  if (!pow2) {
+    if (data_prec(precision) == SSQB_F64) {
+      StftOp<double, double2> op{(const double*)x, window, diff_window, Sfs, bd, N, n_fft,
+                                 hop, n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
+                                 (double2*)Sx, (double2*)dSx, (double*)w, idx, idx_pitch,
+                                 tb.status};
+      e = run_stft_any_f64(op, B, log2M, tb, st);
+    } else {
+      StftOp<float, double2, float2> op{(const float*)x, window, diff_window, Sfs, bd, N,
+                                        n_fft, hop, n1, padtype, s21, modulated ? 1 : 0,
+                                        nframes, gamma, (float2*)Sx, (float2*)dSx,
+                                        (float*)w, idx, idx_pitch, tb.status};
+      e = run_stft_any_f32x(op, B, log2M, tb, st);
+    }
+  } else if (precision == SSQB_F32) {
     StftOp<float, float2> op{(const float*)x, window, diff_window, Sfs, bd, N, n_fft, hop,
                              n1, padtype, s21, modulated ? 1 : 0, nframes, gamma,
                              (float2*)Sx, (float2*)dSx, (float*)w, idx, idx_pitch, tb.status};

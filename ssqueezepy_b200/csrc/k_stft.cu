@@ -23,6 +23,133 @@ static int run_stft(const Op& op, int B, int log2L, const Tables& tb, cudaStream
   });
 }
 
+// ---- any n_fft: Bluestein's chirp-z transform in one kernel -------------------
+// With c_n = e^{-i pi n^2 / L}, the length-L DFT of a frame is
+//   Z_k = c_k (a (*) b)_k,  a_m = z_m c_m (m < L, zero up to M),
+//   b_n = conj(c_n) for n and M - n, 0 <= n < L (zero between),
+// a circular convolution of power-of-two length M >= 2L - 1, so three
+// tile FFTs of M per frame: b's transform, a's transform, and the inverse of
+// their product, all in shared memory; then the Hermitian split of the
+// window / derivative-window pair and the phase / bin epilogue of StftOp.
+// Arithmetic in float64 for every data precision; M <= the float64 tile.
+__device__ __forceinline__ double2 chirp(int n, int L) {
+  // n^2 mod 2L keeps the angle exact before the trigonometric call
+  const long long r = ((long long)n * n) % (2LL * L);
+  double sv, cv;
+  sincospi((double)r / (double)L, &sv, &cv);
+  return make_double2(cv, -sv);
+}
+
+struct NoStore {
+  template <int R>
+  __device__ void item(int, int, int, double2 (&)[R], double2 (&)[R]) const {}
+};
+
+template <typename TX, typename OC, int LOGM>
+__global__ void __launch_bounds__(kNT)
+stft_bluestein_kernel(StftOp<TX, double2, OC> op, Tables tb) {
+  typedef double2 C;
+  typedef typename RealOf<OC>::type OT;
+  constexpr int M = 1 << LOGM;
+  constexpr int NF = tile_of<C>() / M;
+  typedef Layout<C, LOGM, NF> LY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* base = reinterpret_cast<C*>(smem_raw);
+  C* const bufA[1] = {base};
+  C* const bufB[1] = {base + LY::ARR};
+  C* const bufC[1] = {base + 2 * LY::ARR};
+  const int b = blockIdx.z;
+  const int t0 = blockIdx.x * NF;
+  const int L = op.L;
+  const C zero = make_double2(0.0, 0.0);
+  const NoStore st{};
+  // b's transform (the same for every frame of the tile)
+  auto ldB = [&](int, int m, C (&v)[1]) {
+    v[0] = m < L ? chirp(m, L) : (m > M - L ? chirp(M - m, L) : zero);
+    v[0].y = -v[0].y;  // conj(c)
+  };
+  fft_rows<C, LOGM, NF, kNT, -1, 1, MAP_J, MAP_J, false>(bufB, seg_table<C>(tb), ldB, st);
+  // a's transform: the windowed frame times the chirp
+  auto ldA = [&](int f, int m, C (&v)[1]) {
+    const int t = t0 + f;
+    if (t >= op.nframes || m >= L) {
+      v[0] = zero;
+      return;
+    }
+    const int q = op.modulated ? (m + op.s21) % L : m;
+    const long long p = (long long)t * op.hop + q;
+    const int s = pad_src(p - op.n1, op.N, op.padtype);
+    const double xv = s >= 0 ? (double)op.x[(size_t)b * op.N + s] : 0.0;
+    const C z = make_double2(xv * __ldg(op.win + q), xv * __ldg(op.dwin + q));
+    v[0] = cmul(z, chirp(m, L));
+  };
+  fft_rows<C, LOGM, NF, kNT, -1, 1, MAP_J, MAP_J, false>(bufA, seg_table<C>(tb), ldA, st);
+  // inverse transform of the product
+  auto ldC = [&](int f, int m, C (&v)[1]) {
+    v[0] = cmul(bufA[0][LY::at(f, m)], bufB[0][LY::at(f, m)]);
+  };
+  fft_rows<C, LOGM, NF, kNT, 1, 1, MAP_J, MAP_J, false>(bufC, seg_table<C>(tb), ldC, st);
+  const int nrow = (L >> 1) + 1;
+  const double inv_m = 1.0 / M;
+  for (int e = threadIdx.x; e < NF * nrow; e += kNT) {
+    const int f = e % NF, n = e / NF;
+    const int t = t0 + f;
+    if (t >= op.nframes) continue;
+    const int nm = (L - n) % L;
+    C zk = cmul(bufC[0][LY::at(f, n)], chirp(n, L));
+    C zm = cmul(bufC[0][LY::at(f, nm)], chirp(nm, L));
+    zk.x *= inv_m; zk.y *= inv_m;
+    zm.x *= inv_m; zm.y *= inv_m;
+    const double hf = 0.5;
+    const C S = make_double2(hf * (zk.x + zm.x), hf * (zk.y - zm.y));
+    const C dS = make_double2(hf * (zk.y + zm.y), -hf * (zk.x - zm.x));
+    const size_t o = ((size_t)b * nrow + n) * op.nframes + t;
+    if (op.Sx) op.Sx[o] = out_c<OC>(S);
+    if (op.dSx) op.dSx[o] = out_c<OC>(dS);
+    if (op.idx) {
+      double wv;
+      const uint16_t k = phase_bin(S, dS, __ldg(op.sfs + n), true, op.bins, op.gamma,
+                                   op.status, op.w ? &wv : nullptr);
+      op.idx[((size_t)b * nrow + n) * op.idx_pitch + t] = k;
+      if (op.w) op.w[o] = (OT)wv;
+    } else if (op.w) {
+      op.w[o] = (OT)phase_w(S, dS, __ldg(op.sfs + n), true, op.gamma);
+    }
+  }
+}
+
+template <typename TX, typename OC, int LOGM>
+static int launch_bluestein(const StftOp<TX, double2, OC>& op, int B, const Tables& tb,
+                            cudaStream_t st) {
+  constexpr int NF = tile_of<double2>() / (1 << LOGM);
+  const size_t smem = 3 * tile_smem<double2>(1, LOGM);
+  auto k = stft_bluestein_kernel<TX, OC, LOGM>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  dim3 grid((op.nframes + NF - 1) / NF, 1, B);
+  k<<<grid, kNT, smem, st>>>(op, tb);
+  return cudaGetLastError();
+}
+
+template <typename TX, typename OC>
+static int run_bluestein(const StftOp<TX, double2, OC>& op, int B, int log2M,
+                         const Tables& tb, cudaStream_t st) {
+  return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
+    return launch_bluestein<TX, OC, decltype(k)::value>(op, B, tb, st);
+  });
+}
+
+int run_stft_any_f32x(const StftOp<float, double2, float2>& op, int B, int log2M,
+                      const Tables& tb, cudaStream_t st) {
+  return run_bluestein<float, float2>(op, B, log2M, tb, st);
+}
+
+int run_stft_any_f64(const StftOp<double, double2>& op, int B, int log2M, const Tables& tb,
+                     cudaStream_t st) {
+  return run_bluestein<double, double2>(op, B, log2M, tb, st);
+}
+
 int run_stft_f32(const StftOp<float, float2>& op, int B, int log2L, const Tables& tb,
                  cudaStream_t st) {
   return run_stft<StftOp<float, float2>, float2>(op, B, log2L, tb, st);

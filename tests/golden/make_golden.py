@@ -42,9 +42,13 @@ Writes:
                    complex rows (default reflect padding without N, zero
                    padding with N, already padded 2D and 3D input)
 
+  stft_any.npz     stft (Sx, dSx) and ssq_stft (Tx) for n_fft that are not
+                   powers of two (598, 121, 120, 100), modulated on and off,
+                   hop 1 to 4, float64
+
 `--only issq` / `--only ridges` / `--only higher` / `--only istft` /
-`--only difftype` / `--only squeezing` / `--only utils` writes that file
-alone.
+`--only difftype` / `--only squeezing` / `--only utils` / `--only stft_any`
+writes that file alone.
 """
 import os
 import sys
@@ -411,6 +415,30 @@ def utils_fixtures(ref_root):
     np.savez_compressed(os.path.join(HERE, 'utils.npz'), **out)
 
 
+STFT_ANY_CASES = [  # name, N, n_fft, hop, modulated, window
+    ('n598', 600, 598, 4, True, 'hann'),
+    ('n121', 300, 121, 3, True, 'hann'),
+    ('n120', 300, 120, 1, False, 'hann'),
+    ('n100', 300, 100, 2, True, None),
+]
+
+
+def stft_any_fixtures(ref_root):
+    os.environ['SSQ_GPU'] = '0'
+    sys.path.insert(0, ref_root)
+    import ssqueezepy as sq
+    out = {}
+    for name, N, n_fft, hop, mod, win in STFT_ANY_CASES:
+        x = chirp_signal(N, seed=n_fft)
+        Sx, dSx = sq.stft(x, window=win, n_fft=n_fft, hop_len=hop, modulated=mod,
+                          derivative=True, dtype='float64')
+        Tx, *_ = sq.ssq_stft(x, window=win, n_fft=n_fft, hop_len=hop, modulated=mod,
+                             dtype='float64', astensor=False)
+        out[name + '/x'], out[name + '/Sx'] = x, np.asarray(Sx)
+        out[name + '/dSx'], out[name + '/Tx'] = np.asarray(dSx), np.asarray(Tx)
+    np.savez_compressed(os.path.join(HERE, 'stft_any.npz'), **out)
+
+
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
     root = args[0] if args else '/root/reference'
@@ -428,6 +456,8 @@ if __name__ == '__main__':
         squeezing_fixtures(root)
     elif '--only' in sys.argv and 'utils' in sys.argv:
         utils_fixtures(root)
+    elif '--only' in sys.argv and 'stft_any' in sys.argv:
+        stft_any_fixtures(root)
     else:
         main(root)
         issq_fixtures(root)
@@ -437,3 +467,4 @@ if __name__ == '__main__':
         difftype_fixtures(root)
         squeezing_fixtures(root)
         utils_fixtures(root)
+        stft_any_fixtures(root)

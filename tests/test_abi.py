@@ -80,8 +80,11 @@ def test_other_entry_points_reject_bad_arguments():
     assert lib.ssqb_ssqueeze_fast(p, p, None, p, None, 1e-6, 1, 5, 5, 0, p, None) \
         == L.EINVAL
     b = L.make_bins(2, (0., 0.1, 0, 0, 0), 65, 0)
-    assert lib.ssqb_stft(p, 1, 100, 100, 1, 50, 1, 1, p, p, p, b, 1e-6, 0, p, None,
-                         None, None, 0, None) == L.EUNSUPPORTED
+    # lengths past the chirp-z range (not a power of two and above 1024, or
+    # below 4) are refused before any device work
+    for n_fft in (1025, 2000, 3):
+        assert lib.ssqb_stft(p, 1, 100, n_fft, 1, 50, 1, 1, p, p, p, b, 1e-6, 0, p, None,
+                             None, None, 0, None) == L.EUNSUPPORTED, n_fft
     assert lib.ssqb_stft(p, 1, 100, 128, 0, 64, 1, 1, p, p, p, b, 1e-6, 0, p, None,
                          None, None, 0, None) == L.EINVAL
     assert lib.ssqb_icwt(None, p, None, 1.0, 1, 10, 10, 0, p, None) == L.EINVAL
