@@ -59,16 +59,19 @@ stft_bluestein_kernel(StftOp<TX, double2, OC> op, Tables tb) {
   C* const bufB[1] = {base + LY::ARR};
   C* const bufC[1] = {base + 2 * LY::ARR};
   const int b = blockIdx.z;
-  const int t0 = blockIdx.x * NF;
   const int L = op.L;
   const C zero = make_double2(0.0, 0.0);
   const NoStore st{};
-  // b's transform (the same for every frame of the tile)
+  // b's transform, the same for every frame: once per CTA, which then walks
+  // the tiles of frames blockIdx.x, blockIdx.x + gridDim.x, ...
   auto ldB = [&](int, int m, C (&v)[1]) {
     v[0] = m < L ? chirp(m, L) : (m > M - L ? chirp(M - m, L) : zero);
     v[0].y = -v[0].y;  // conj(c)
   };
   fft_rows<C, LOGM, NF, kNT, -1, 1, MAP_J, MAP_J, false>(bufB, seg_table<C>(tb), ldB, st);
+  const int ntile = (op.nframes + NF - 1) / NF;
+  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+  const int t0 = tile * NF;
   // a's transform: the windowed frame times the chirp
   auto ldA = [&](int f, int m, C (&v)[1]) {
     const int t = t0 + f;
@@ -116,6 +119,8 @@ stft_bluestein_kernel(StftOp<TX, double2, OC> op, Tables tb) {
       op.w[o] = (OT)phase_w(S, dS, __ldg(op.sfs + n), true, op.gamma);
     }
   }
+  __syncthreads();  // bufC is rewritten by the next tile
+  }
 }
 
 template <typename TX, typename OC, int LOGM>
@@ -127,7 +132,20 @@ static int launch_bluestein(const StftOp<TX, double2, OC>& op, int B, const Tabl
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e) return e;
-  dim3 grid((op.nframes + NF - 1) / NF, 1, B);
+  // persistent CTAs: as many as are resident (at most one per tile of frames)
+  int dev = 0, sms = 148, per_sm = 1;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kNT, smem) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+    per_sm = 1;
+  }
+  const int ntile = (op.nframes + NF - 1) / NF;
+  int gx = sms * (per_sm > 0 ? per_sm : 1);
+  if (B > 1) gx = (gx + B - 1) / B;
+  if (gx > ntile) gx = ntile;
+  dim3 grid(gx, 1, B);
   k<<<grid, kNT, smem, st>>>(op, tb);
   return cudaGetLastError();
 }
