@@ -364,7 +364,8 @@ SSQB_API size_t ssqb_istft_workspace_bytes(int B, int n_fft, int n_frames, int p
  * normal number of the data type, _stft.py:245-250), and unpadded by
  * n_fft/2 samples on the left. Sx (B, n_fft/2+1, n_frames); wa, w1 (n_fft)
  * double; x (B, N) real. The frames must end inside the padded signal:
- * (n_frames - 1) * hop <= N - 1. */
+ * (n_frames - 1) * hop <= N - 1. n_fft a power of two <= 4096, or any length
+ * in [4, 1024] (the frames by Bluestein's chirp-z transform, float64). */
 SSQB_API int ssqb_istft(const void* Sx, int B, int n_fft, int n_frames, int hop, int N,
                         int modulated, const double* wa, const double* w1, double tiny,
                         int precision, void* x, void* workspace, size_t workspace_bytes,

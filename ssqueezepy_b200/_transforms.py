@@ -1074,9 +1074,11 @@ def istft(Sx, window=None, n_fft=None, win_len=None, hop_len=1, N=None,
     win_len = win_len or n_fft
     N = N or hop_len * nframes
     dtype = 'float32' if S.dtype == torch.complex64 else 'float64'
-    if n_fft & (n_fft - 1) or n_fft < 8 or n_fft > 4096:
-        raise NotImplementedError("n_fft must be a power of two in [8, 4096] on "
-                                  "the accelerated path (got %s)" % n_fft)
+    if (n_fft & (n_fft - 1) == 0 and not 8 <= n_fft <= 4096) or \
+            (n_fft & (n_fft - 1) and not 4 <= n_fft <= 1024):
+        raise NotImplementedError("n_fft must be a power of two in [8, 4096] or any "
+                                  "length in [4, 1024] on the accelerated path "
+                                  "(got %s)" % n_fft)
     if nrow != n_fft // 2 + 1:
         raise NotImplementedError("`Sx` must have n_fft//2 + 1 rows on the "
                                   "accelerated path (got %s for n_fft=%s)" % (nrow, n_fft))

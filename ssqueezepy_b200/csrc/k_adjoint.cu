@@ -204,6 +204,7 @@ __global__ void istft_ola_kernel(const T* __restrict__ gu, const double* __restr
   const int b = (int)(i / N), s = (int)(i % N);
   const T* g = gu + (size_t)b * L * nframes;
   const int half = L / 2;
+  const int shift = (L + 1) / 2;  // fftshift: frame index m of padded offset q
   const long long p = (long long)s + half;
   const long long num = p - L + 1;
   const long long tlo = num <= 0 ? 0 : (num + hop - 1) / hop;
@@ -213,7 +214,7 @@ __global__ void istft_ola_kernel(const T* __restrict__ gu, const double* __restr
   double acc = 0.0, wn = 0.0;
   for (long long t = tlo; t <= thi; ++t) {
     const int q = (int)(p - t * hop);
-    const int m = modulated ? ((q + half) & (L - 1)) : q;
+    const int m = modulated ? (q + shift) % L : q;
     acc += (double)g[(size_t)m * nframes + t] * wa[q];
   }
   for (long long t = tlo; t <= tw; ++t) wn += w1[(int)(p - t * hop)];
@@ -228,10 +229,20 @@ static int run_istft(const C* Sx, int B, int N, int L, int hop, int nframes, int
                      cudaStream_t st) {
   typedef typename RealOf<C>::type T;
   const int nrow = L / 2 + 1;
-  AdjSources<C> src{Sx, nullptr, nullptr, 0, nrow, nullptr, nullptr, nullptr};
-  StftAdjOp<C> op{src, L, nrow, nframes, (T*)ws, tb.status, 1};
-  int e = run_single<StftAdjOp<C>, C, 1>(op, B, nframes, ilog2(L), tb, st);
-  if (e) return e;
+  int e;
+  if (L & (L - 1)) {  // not a power of two: frames by the chirp-z kernel
+    if constexpr (std::is_same<C, double2>::value)
+      e = run_istft_frames_any_f64(Sx, B, L, nframes, (double*)ws, tb, st);
+    else
+      e = run_istft_frames_any_f32(Sx, B, L, nframes, (float*)ws, tb, st);
+    if (e) return e;
+    if (int* c = launch_counter()) return ++*c, 0;
+  } else {
+    AdjSources<C> src{Sx, nullptr, nullptr, 0, nrow, nullptr, nullptr, nullptr};
+    StftAdjOp<C> op{src, L, nrow, nframes, (T*)ws, tb.status, 1};
+    e = run_single<StftAdjOp<C>, C, 1>(op, B, nframes, ilog2(L), tb, st);
+    if (e) return e;
+  }
   if (int* c = launch_counter()) return ++*c, 0;
   const int maxhops = (N - 1) / hop + 1;
   const size_t n = (size_t)B * N;

@@ -158,6 +158,111 @@ static int run_bluestein(const StftOp<TX, double2, OC>& op, int B, int log2M,
   });
 }
 
+// ---- istft frames for any n_fft: the inverse real transform by chirp-z ------
+// y_m = sum_k X_k e^{+2 pi i k m / L} = conj(c_m) (a' (*) c)_m with
+// a'_k = X_k conj(c_k), X_k = c_k' S_k for k <= L/2 (c_k' = 1 at k = 0 and
+// k = L/2, else 2: the one-sided spectrum of a real frame), 0 above; the
+// frame is Re y (1/L is applied by the overlap-add). Frames go to gu
+// (B, L, nframes), element-major, as the power-of-two path writes them.
+template <typename CI, typename T, int LOGM>
+__global__ void __launch_bounds__(kNT)
+istft_frames_bluestein_kernel(const CI* __restrict__ Sx, int L, int nframes,
+                              T* __restrict__ gu, Tables tb) {
+  typedef double2 C;
+  constexpr int M = 1 << LOGM;
+  constexpr int NF = tile_of<C>() / M;
+  typedef Layout<C, LOGM, NF> LY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* base = reinterpret_cast<C*>(smem_raw);
+  C* const bufA[1] = {base};
+  C* const bufB[1] = {base + LY::ARR};
+  C* const bufC[1] = {base + 2 * LY::ARR};
+  const int b = blockIdx.z;
+  const int nrow = L / 2 + 1;
+  const C zero = make_double2(0.0, 0.0);
+  const NoStore st{};
+  auto ldB = [&](int, int m, C (&v)[1]) {
+    v[0] = m < L ? chirp(m, L) : (m > M - L ? chirp(M - m, L) : zero);
+  };
+  fft_rows<C, LOGM, NF, kNT, -1, 1, MAP_J, MAP_J, false>(bufB, seg_table<C>(tb), ldB, st);
+  const int ntile = (nframes + NF - 1) / NF;
+  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const int t0 = tile * NF;
+    auto ldA = [&](int f, int k, C (&v)[1]) {
+      const int t = t0 + f;
+      if (t >= nframes || k >= nrow) {
+        v[0] = zero;
+        return;
+      }
+      const CI sv = Sx[((size_t)b * nrow + k) * nframes + t];
+      const double wk = (k == 0 || 2 * k == L) ? 1.0 : 2.0;
+      C c = chirp(k, L);
+      c.y = -c.y;
+      v[0] = cmul(make_double2(wk * (double)sv.x, wk * (double)sv.y), c);
+    };
+    fft_rows<C, LOGM, NF, kNT, -1, 1, MAP_J, MAP_J, false>(bufA, seg_table<C>(tb), ldA, st);
+    auto ldC = [&](int f, int m, C (&v)[1]) {
+      v[0] = cmul(bufA[0][LY::at(f, m)], bufB[0][LY::at(f, m)]);
+    };
+    fft_rows<C, LOGM, NF, kNT, 1, 1, MAP_J, MAP_J, false>(bufC, seg_table<C>(tb), ldC, st);
+    for (int e = threadIdx.x; e < NF * L; e += kNT) {
+      const int f = e % NF, m = e / NF;
+      const int t = t0 + f;
+      if (t >= nframes) continue;
+      C c = chirp(m, L);
+      c.y = -c.y;
+      const C y = cmul(bufC[0][LY::at(f, m)], c);
+      gu[((size_t)b * L + m) * nframes + t] = (T)(y.x / M);
+    }
+    __syncthreads();  // bufA / bufC are rewritten by the next tile
+  }
+}
+
+template <typename CI, typename T, int LOGM>
+static int launch_istft_frames(const CI* Sx, int B, int L, int nframes, T* gu,
+                               const Tables& tb, cudaStream_t st) {
+  constexpr int NF = tile_of<double2>() / (1 << LOGM);
+  const size_t smem = 3 * tile_smem<double2>(1, LOGM);
+  auto k = istft_frames_bluestein_kernel<CI, T, LOGM>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kNT, smem) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+    per_sm = 1;
+  }
+  const int ntile = (nframes + NF - 1) / NF;
+  int gx = sms * (per_sm > 0 ? per_sm : 1);
+  if (B > 1) gx = (gx + B - 1) / B;
+  if (gx > ntile) gx = ntile;
+  k<<<dim3(gx, 1, B), kNT, smem, st>>>(Sx, L, nframes, gu, tb);
+  return cudaGetLastError();
+}
+
+int run_istft_frames_any_f32(const float2* Sx, int B, int L, int nframes, float* gu,
+                             const Tables& tb, cudaStream_t st) {
+  int log2M = 0;
+  while ((1 << log2M) < 2 * L - 1) ++log2M;
+  return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
+    return launch_istft_frames<float2, float, decltype(k)::value>(Sx, B, L, nframes, gu, tb,
+                                                                  st);
+  });
+}
+
+int run_istft_frames_any_f64(const double2* Sx, int B, int L, int nframes, double* gu,
+                             const Tables& tb, cudaStream_t st) {
+  int log2M = 0;
+  while ((1 << log2M) < 2 * L - 1) ++log2M;
+  return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
+    return launch_istft_frames<double2, double, decltype(k)::value>(Sx, B, L, nframes, gu,
+                                                                    tb, st);
+  });
+}
+
 int run_stft_any_f32x(const StftOp<float, double2, float2>& op, int B, int log2M,
                       const Tables& tb, cudaStream_t st) {
   return run_bluestein<float, float2>(op, B, log2M, tb, st);

@@ -305,6 +305,11 @@ ISTFT_CASES = [
     ('e', 300, 64, 64, 1, 'hann', 300, True, 1, 'float32'),
     ('f', 600, 512, 512, 4, 'hann', 600, True, 1, 'float64'),
     ('g', 1000, 128, 100, 5, 'hamming', 997, False, 1, 'float64'),
+    # n_fft not a power of two (the reference's benchmark length, odd, even)
+    ('h', 600, 598, 598, 4, 'hann', 600, True, 1, 'float64'),
+    ('i', 300, 121, 121, 3, 'hann', 300, True, 1, 'float64'),
+    ('j', 300, 100, 90, 2, 'hann', 300, False, 0, 'float64'),
+    ('k', 300, 121, 121, 1, 'hann', 300, True, 1, 'float32'),
 ]
 
 

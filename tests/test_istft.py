@@ -41,7 +41,7 @@ def test_istft_argument_checks():
     with pytest.raises(ValueError):
         sb.istft(S.real)
     with pytest.raises(NotImplementedError):
-        sb.istft(S, n_fft=48)           # not a power of two
+        sb.istft(S, n_fft=2000)         # not a power of two, above 1024
     with pytest.raises(NotImplementedError):
         sb.istft(S, n_fft=128)          # rows != n_fft//2 + 1
     with pytest.raises(ValueError):
@@ -61,7 +61,8 @@ def test_istft_abi_rejects_bad_arguments():
                               a['ws'], a['wsb'], None)
     assert call(S=None) == L.EINVAL
     assert call(B=0) == L.EINVAL
-    assert call(n_fft=48) == L.EUNSUPPORTED
+    assert call(n_fft=2000) == L.EUNSUPPORTED      # not a power of two, above 1024
+    assert call(n_fft=3) == L.EUNSUPPORTED
     assert call(n_fft=8192) == L.EUNSUPPORTED
     assert call(nf=11) == L.EINVAL                # (11 - 1) * 1 > 9
     assert call(tiny=-1.) == L.EINVAL
