@@ -751,7 +751,7 @@ int ssqb_cwt_adjoint(const void* gWx, const void* gTx, const uint16_t* idx, int 
 }
 
 size_t ssqb_stft_adjoint_workspace_bytes(int B, int N, int n_fft, int hop, int precision) {
-  if (B < 1 || N < 1 || hop < 1 || !is_pow2(n_fft) || !valid_precision(precision)) return 0;
+  if (B < 1 || N < 1 || hop < 1 || n_fft < 1 || !valid_precision(precision)) return 0;
   const size_t rs = data_prec(precision) == SSQB_F64 ? sizeof(double) : sizeof(float);
   return (size_t)B * n_fft * ((size_t)(N - 1) / hop + 1) * rs;
 }
@@ -766,10 +766,16 @@ int ssqb_stft_adjoint(const void* gSx, const void* gTx, const uint16_t* idx, int
   if (B > 65535) return fail(SSQB_EINVAL, "B must be <= 65535");
   if (!valid_precision(precision))
     return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
-  if (!is_pow2(n_fft) || n_fft < 8 || n_fft > 4096)
-    return fail(SSQB_EUNSUPPORTED, "n_fft must be a power of two in [8, 4096]");
+  const bool pow2 = is_pow2(n_fft);
+  int log2M = 0;
+  while ((1 << log2M) < 2 * n_fft - 1) ++log2M;
+  if (pow2 ? (n_fft < 8 || n_fft > 4096)
+           : (n_fft < 4 || (1 << log2M) > FftCfg<double2>::TILE))
+    return fail(SSQB_EUNSUPPORTED,
+                "n_fft must be a power of two in [8, 4096] or any length in [4, " +
+                    std::to_string((FftCfg<double2>::TILE + 1) / 2) + "]");
   const bool f64 = data_prec(precision) == SSQB_F64;
-  if (f64 && n_fft > FftCfg<double2>::TILE)
+  if (pow2 && f64 && n_fft > FftCfg<double2>::TILE)
     return fail(SSQB_EUNSUPPORTED, "n_fft above " + std::to_string(FftCfg<double2>::TILE) +
                                        " needs float32 data");
   if (padtype < 0 || padtype > 5) return fail(SSQB_EINVAL, "unknown padtype");

@@ -174,7 +174,7 @@ __global__ void stft_adj_gather_kernel(const T* __restrict__ gu, const double* _
     if (thi > nframes - 1) thi = nframes - 1;
     for (long long t = thi; t >= tlo; --t) {
       const int q = (int)(p - t * hop);
-      const int m = modulated ? ((q - s21) & (L - 1)) : q;
+      const int m = modulated ? ((q - s21) % L + L) % L : q;
       acc += (T)__ldg(win + q) * g[(size_t)m * nframes + t];
     }
   });
@@ -346,8 +346,16 @@ static int run_stft_adj(const AdjSources<C>& src, int B, int N, int L, int hop, 
                         const Tables& tb, cudaStream_t st) {
   typedef typename RealOf<C>::type T;
   const int nframes = (N - 1) / hop + 1;
-  StftAdjOp<C> op{src, L, L / 2 + 1, nframes, (T*)ws, tb.status, 0};
-  int e = run_single<StftAdjOp<C>, C, 1>(op, B, nframes, ilog2(L), tb, st);
+  int e;
+  if (L & (L - 1)) {  // not a power of two: the chirp-z frame transform
+    if constexpr (std::is_same<C, double2>::value)
+      e = run_adj_frames_any_f64(src, B, L, nframes, (double*)ws, tb, st);
+    else
+      e = run_adj_frames_any_f32(src, B, L, nframes, (float*)ws, tb, st);
+  } else {
+    StftAdjOp<C> op{src, L, L / 2 + 1, nframes, (T*)ws, tb.status, 0};
+    e = run_single<StftAdjOp<C>, C, 1>(op, B, nframes, ilog2(L), tb, st);
+  }
   if (e) return e;
   if (int* c = launch_counter()) return ++*c, 0;
   const int s20 = (L + 1) / 2;

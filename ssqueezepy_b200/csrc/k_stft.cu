@@ -164,10 +164,30 @@ static int run_bluestein(const StftOp<TX, double2, OC>& op, int B, int log2M,
 // k = L/2, else 2: the one-sided spectrum of a real frame), 0 above; the
 // frame is Re y (1/L is applied by the overlap-add). Frames go to gu
 // (B, L, nframes), element-major, as the power-of-two path writes them.
-template <typename CI, typename T, int LOGM>
+// One-sided inputs of the frame transform: the spectrum of istft (interior
+// bins doubled), or the gradient sources of the STFT adjoint (weights 1).
+template <typename CI>
+struct SpecSrc {
+  const CI* Sx;
+  __device__ double2 at(int b, int nrow, int nframes, int k, int t, int L) const {
+    const CI sv = Sx[((size_t)b * nrow + k) * nframes + t];
+    const double wk = (k == 0 || 2 * k == L) ? 1.0 : 2.0;
+    return make_double2(wk * (double)sv.x, wk * (double)sv.y);
+  }
+};
+template <typename CI>
+struct AdjSrc {
+  AdjSources<CI> src;
+  int* status;
+  __device__ double2 at(int b, int nrow, int nframes, int k, int t, int) const {
+    const CI v = src.at(b, nrow, nframes, k, t, status);
+    return make_double2((double)v.x, (double)v.y);
+  }
+};
+
+template <class Src, typename T, int LOGM>
 __global__ void __launch_bounds__(kNT)
-istft_frames_bluestein_kernel(const CI* __restrict__ Sx, int L, int nframes,
-                              T* __restrict__ gu, Tables tb) {
+istft_frames_bluestein_kernel(Src src, int L, int nframes, T* __restrict__ gu, Tables tb) {
   typedef double2 C;
   constexpr int M = 1 << LOGM;
   constexpr int NF = tile_of<C>() / M;
@@ -194,11 +214,9 @@ istft_frames_bluestein_kernel(const CI* __restrict__ Sx, int L, int nframes,
         v[0] = zero;
         return;
       }
-      const CI sv = Sx[((size_t)b * nrow + k) * nframes + t];
-      const double wk = (k == 0 || 2 * k == L) ? 1.0 : 2.0;
       C c = chirp(k, L);
       c.y = -c.y;
-      v[0] = cmul(make_double2(wk * (double)sv.x, wk * (double)sv.y), c);
+      v[0] = cmul(src.at(b, nrow, nframes, k, t, L), c);
     };
     fft_rows<C, LOGM, NF, kNT, -1, 1, MAP_J, MAP_J, false>(bufA, seg_table<C>(tb), ldA, st);
     auto ldC = [&](int f, int m, C (&v)[1]) {
@@ -218,12 +236,12 @@ istft_frames_bluestein_kernel(const CI* __restrict__ Sx, int L, int nframes,
   }
 }
 
-template <typename CI, typename T, int LOGM>
-static int launch_istft_frames(const CI* Sx, int B, int L, int nframes, T* gu,
+template <class Src, typename T, int LOGM>
+static int launch_istft_frames(const Src& src, int B, int L, int nframes, T* gu,
                                const Tables& tb, cudaStream_t st) {
   constexpr int NF = tile_of<double2>() / (1 << LOGM);
   const size_t smem = 3 * tile_smem<double2>(1, LOGM);
-  auto k = istft_frames_bluestein_kernel<CI, T, LOGM>;
+  auto k = istft_frames_bluestein_kernel<Src, T, LOGM>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e) return e;
@@ -239,28 +257,38 @@ static int launch_istft_frames(const CI* Sx, int B, int L, int nframes, T* gu,
   int gx = sms * (per_sm > 0 ? per_sm : 1);
   if (B > 1) gx = (gx + B - 1) / B;
   if (gx > ntile) gx = ntile;
-  k<<<dim3(gx, 1, B), kNT, smem, st>>>(Sx, L, nframes, gu, tb);
+  k<<<dim3(gx, 1, B), kNT, smem, st>>>(src, L, nframes, gu, tb);
   return cudaGetLastError();
+}
+
+template <class Src, typename T>
+static int run_frames_any(const Src& src, int B, int L, int nframes, T* gu, const Tables& tb,
+                          cudaStream_t st) {
+  int log2M = 0;
+  while ((1 << log2M) < 2 * L - 1) ++log2M;
+  return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
+    return launch_istft_frames<Src, T, decltype(k)::value>(src, B, L, nframes, gu, tb, st);
+  });
 }
 
 int run_istft_frames_any_f32(const float2* Sx, int B, int L, int nframes, float* gu,
                              const Tables& tb, cudaStream_t st) {
-  int log2M = 0;
-  while ((1 << log2M) < 2 * L - 1) ++log2M;
-  return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
-    return launch_istft_frames<float2, float, decltype(k)::value>(Sx, B, L, nframes, gu, tb,
-                                                                  st);
-  });
+  return run_frames_any(SpecSrc<float2>{Sx}, B, L, nframes, gu, tb, st);
 }
 
 int run_istft_frames_any_f64(const double2* Sx, int B, int L, int nframes, double* gu,
                              const Tables& tb, cudaStream_t st) {
-  int log2M = 0;
-  while ((1 << log2M) < 2 * L - 1) ++log2M;
-  return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
-    return launch_istft_frames<double2, double, decltype(k)::value>(Sx, B, L, nframes, gu,
-                                                                    tb, st);
-  });
+  return run_frames_any(SpecSrc<double2>{Sx}, B, L, nframes, gu, tb, st);
+}
+
+int run_adj_frames_any_f32(const AdjSources<float2>& src, int B, int L, int nframes,
+                           float* gu, const Tables& tb, cudaStream_t st) {
+  return run_frames_any(AdjSrc<float2>{src, tb.status}, B, L, nframes, gu, tb, st);
+}
+
+int run_adj_frames_any_f64(const AdjSources<double2>& src, int B, int L, int nframes,
+                           double* gu, const Tables& tb, cudaStream_t st) {
+  return run_frames_any(AdjSrc<double2>{src, tb.status}, B, L, nframes, gu, tb, st);
 }
 
 int run_stft_any_f32x(const StftOp<float, double2, float2>& op, int B, int log2M,

@@ -75,6 +75,10 @@ int run_istft_frames_any_f32(const float2* Sx, int B, int L, int nframes, float*
                              const Tables& tb, cudaStream_t st);
 int run_istft_frames_any_f64(const double2* Sx, int B, int L, int nframes, double* gu,
                              const Tables& tb, cudaStream_t st);
+int run_adj_frames_any_f32(const AdjSources<float2>& src, int B, int L, int nframes,
+                           float* gu, const Tables& tb, cudaStream_t st);
+int run_adj_frames_any_f64(const AdjSources<double2>& src, int B, int L, int nframes,
+                           double* gu, const Tables& tb, cudaStream_t st);
 int run_stft_any_f32x(const StftOp<float, double2, float2>& op, int B, int log2M,
                       const Tables& tb, cudaStream_t st);
 int run_stft_any_f64(const StftOp<double, double2>& op, int B, int log2M, const Tables& tb,

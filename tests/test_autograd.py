@@ -263,6 +263,30 @@ def test_stft_backward_matches_oracle_adjoint(dtype, hop, padtype):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+@pytest.mark.parametrize('n_fft, hop', [(121, 1), (100, 2), (598, 3)])
+def test_stft_backward_any_length_matches_oracle_adjoint(dtype, n_fft, hop):
+    """n_fft not a power of two: the frame transform of the backward goes
+    through the chirp-z kernel, the gather rotates modulo n_fft."""
+    torch = _torch()
+    import ssqueezepy_b200 as sb
+    from oracle import ssq_oracle as O
+    from scipy.signal import get_window
+    N = 1500
+    rng = np.random.default_rng(n_fft)
+    x = torch.tensor(S.same_length_batch(2, N, 5), device='cuda',
+                     dtype=getattr(torch, dtype), requires_grad=True)
+    Sx = sb.stft(x, window='hann', n_fft=n_fft, hop_len=hop, dtype=dtype)
+    g = rng.standard_normal(Sx.shape) + 1j * rng.standard_normal(Sx.shape)
+    (gx,) = torch.autograd.grad(Sx, x, torch.as_tensor(g, dtype=Sx.dtype, device='cuda'))
+    win = get_window('hann', n_fft, fftbins=True)
+    ref = O.stft_adjoint(g, win, n_fft, N, hop=hop)
+    err = np.linalg.norm(gx.double().cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err <= (1e-5 if dtype == 'float32' else 1e-11), err
+    assert L.device_status() == 0
+
+
+@pytest.mark.gpu
 def test_ssq_stft_backward_is_gather_then_transpose():
     torch = _torch()
     import ssqueezepy_b200 as sb

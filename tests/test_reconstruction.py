@@ -4,8 +4,8 @@ the path (tests/reconstruction_test.py), on the GPU: transform -> inverse
 returns the signal within the reference's thresholds on its test-signal
 families (exponential and linear chirps, fast frequency transitions, low and
 high frequencies). The metric is mean |x - xrec| / rms(x)
-(reconstruction_test.py:28-31). STFT cases use a power-of-two n_fft (128)
-where the reference uses 120 / 121: this package's STFT takes powers of two."""
+(reconstruction_test.py:28-31). The STFT cases take the reference's n_fft
+of 120 and 121 (through the chirp-z kernels) and 128."""
 import numpy as np
 import pytest
 
@@ -129,12 +129,13 @@ def test_component_inversion():
 
 
 @pytest.mark.parametrize('N', [128, 129])
+@pytest.mark.parametrize('n_fft', [120, 121, 128])
 @pytest.mark.parametrize('hop_len', [1, 2, 3])
 @pytest.mark.parametrize('modulated', [True, False])
-def test_stft_istft_inverts(N, hop_len, modulated):
+def test_stft_istft_inverts(N, n_fft, hop_len, modulated):
     sb = _gpu()
     x = np.random.default_rng(N + hop_len).standard_normal(N)
-    kw = dict(hop_len=hop_len, n_fft=128, modulated=modulated)
+    kw = dict(hop_len=hop_len, n_fft=n_fft, modulated=modulated)
     Sx = sb.stft(x, dtype='float64', **kw)
     xr = sb.istft(Sx, N=len(x), **kw).cpu().numpy()
     assert len(xr) == N
@@ -142,14 +143,15 @@ def test_stft_istft_inverts(N, hop_len, modulated):
 
 
 @pytest.mark.parametrize('N', [128, 129])
+@pytest.mark.parametrize('n_fft', [120, 121])
 @pytest.mark.parametrize('window_scaling', [1., .5])
-def test_ssq_stft_inverts(N, window_scaling):
+def test_ssq_stft_inverts(N, n_fft, window_scaling):
     sb = _gpu()
     x = np.random.default_rng(N).standard_normal(N)
     window = None
     if window_scaling != 1:
-        window = sb.get_window(None, win_len=128, n_fft=128) * window_scaling
-    Tx, *_ = sb.ssq_stft(x, window=window, n_fft=128, astensor=False)
-    xr = np.asarray(sb.issq_stft(Tx, window=window, n_fft=128))
+        window = sb.get_window(None, win_len=n_fft, n_fft=n_fft) * window_scaling
+    Tx, *_ = sb.ssq_stft(x, window=window, n_fft=n_fft, astensor=False)
+    xr = np.asarray(sb.issq_stft(Tx, window=window, n_fft=n_fft))
     assert len(xr) == N
     assert np.abs(x - xr).mean() < .1
