@@ -99,8 +99,8 @@ def _default_gamma(dtype):
 
 
 def _dev_f64(a, dev):
-    return torch.as_tensor(np.ascontiguousarray(np.asarray(a, np.float64).ravel()),
-                           device=dev)
+    # a copy: read-only inputs (np.load, broadcast views) give writable memory
+    return torch.as_tensor(np.array(a, dtype=np.float64).ravel(), device=dev)
 
 
 #### host parameter cache ###################################################
