@@ -105,6 +105,12 @@ class Clocks:
             self.th.start()
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi's start-up (NVML initialisation) stalls kernel launches
+        # for milliseconds: let it finish before any timed step
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < 10 and self.proc.poll() is None:
+            time.sleep(0.05)
 
     def _read(self):
         for line in self.proc.stdout:
