@@ -1,8 +1,9 @@
 // Phase transforms by differences along time: difftype 'phase' (the
 // unwrapped angle of Wx, _ssq_cwt.py:490-496) and difftype 'numeric'
 // (phase_cwt_num, _ssq_cwt.py:512-586). Both read one row segment of Wx per
-// (signal, scale) and write w of the same width; both are HBM-bound
-// elementwise passes (16 or 8 bytes read and 8 or 4 written per element).
+// (signal, scale) and write w of the same width (16 or 8 bytes read and 8 or 4
+// written per element); the unwrap is bound by its float64 atan2, one per
+// element, the numeric differences by HBM.
 #include <cmath>
 #include "launch.h"
 
@@ -12,7 +13,7 @@ namespace {
 
 constexpr double kPi = 3.141592653589793;
 constexpr double kTwoPiPhase = 6.283185307179586;
-constexpr int kPhaseThreads = 256;
+constexpr int kPhaseThreads = 512;
 
 // numpy's unwrap correction of one angle difference (period 2 pi, discont
 // pi): differences below pi in size are kept; others are moved into
@@ -34,24 +35,39 @@ __device__ __forceinline__ double cabs_d(C v) {
 
 // One CTA per row: w[j] = |step_j| / 2pi for j < M-1, and for the last
 // column the size of the whole unwrapped excursion u[M-1] - u[0], the sum of
-// the steps (block tree reduction in a fixed order, so deterministic).
+// the steps (block tree reduction in a fixed order, so deterministic). The
+// angles of a tile of columns (plus the next tile's first) are staged in
+// shared memory, so each angle is computed once.
 template <typename C>
 __global__ void __launch_bounds__(kPhaseThreads)
 phase_unwrap_kernel(const C* __restrict__ Wx, int ncol, int col0, int M, double gamma,
                     typename RealOf<C>::type* __restrict__ w) {
   typedef typename RealOf<C>::type T;
   __shared__ double part[kPhaseThreads];
+  __shared__ double ang[kPhaseThreads + 1];
   const size_t r = blockIdx.x;
   const C* W = Wx + r * (size_t)ncol + col0;
   T* out = w + r * (size_t)M;
+  const int tid = threadIdx.x;
   double acc = 0.0;
-  for (int j = threadIdx.x; j < M - 1; j += blockDim.x) {
-    const C a = W[j], b = W[j + 1];
-    const double pa = atan2((double)a.y, (double)a.x);
-    const double pb = atan2((double)b.y, (double)b.x);
-    const double d = unwrap_step(pb - pa);
-    acc += d;
-    out[j] = cabs_d(a) < gamma ? (T)INFINITY : (T)(fabs(d) / kTwoPiPhase);
+  for (int j0 = 0; j0 < M - 1; j0 += kPhaseThreads) {
+    const int j = j0 + tid;
+    C a = W[0];
+    if (j < M) {
+      a = W[j];
+      ang[tid] = atan2((double)a.y, (double)a.x);
+    }
+    if (tid == 0 && j0 + kPhaseThreads < M) {
+      const C b = W[j0 + kPhaseThreads];
+      ang[kPhaseThreads] = atan2((double)b.y, (double)b.x);
+    }
+    __syncthreads();
+    if (j < M - 1) {
+      const double d = unwrap_step(ang[tid + 1] - ang[tid]);
+      acc += d;
+      out[j] = cabs_d(a) < gamma ? (T)INFINITY : (T)(fabs(d) / kTwoPiPhase);
+    }
+    __syncthreads();  // ang is rewritten by the next tile
   }
   part[threadIdx.x] = acc;
   __syncthreads();
