@@ -169,9 +169,12 @@ SSQB_API int ssqb_stft(const void* x, int B, int N, int n_fft, int hop, int n1, 
  * scales, Wx, idx, ...); the padded-signal spectrum and the two-pass
  * intermediate live in one fixed scratch array of ssqb_cwt_noalloc_max_bytes()
  * (16 MiB) of module memory that every device loading the library holds
- * until the process exits. A call needing more (roughly B * Npad * 48 bytes
- * for Npad > 2048 with float64 arithmetic, B * Npad * 16 otherwise) fails
- * with SSQB_EINVAL and a message naming the size. The first call on a device
+ * until the process exits. A call needs B * Npad * 16 bytes for Npad <= 2048;
+ * above that B * Npad * 48 bytes with float64 arithmetic (SSQB_F64,
+ * SSQB_F32X) and B * Npad * 32 bytes with SSQB_F32. A call needing more
+ * fails with SSQB_EINVAL and a message naming the size; the exact figure is
+ * the minimum ssqb_cwt would accept, and ssqb_cwt_noalloc_max_bytes() gives
+ * the limit. The first call on a device
  * looks up the array's device address (and builds the twiddle tables); make
  * that first call before any stream capture. Nothing is allocated or freed.
  * All calls share the one array: calls that overlap on the GPU (other

@@ -258,6 +258,60 @@ def bin_index(w, ssq_freqs, logscale, flipud):
     return k
 
 
+def bin_edge_w(w, ssq_freqs, logscale):
+    """Phase-transform value of the rounding edge nearest to each `w` under
+    the bin rule of `bin_index` (algos.py:859-953), and of the split of a
+    log-piecewise grid where that is nearer."""
+    v = np.asarray(ssq_freqs, np.float64).ravel()
+    with np.errstate(divide='ignore', invalid='ignore'):
+        if not logscale:
+            dv = max(float(v[1] - v[0]), EPS64)
+            e = np.floor((w - v[0]) / dv) + .5
+            return v[0] + e * dv
+        wl = np.log2(w)
+        idx = transition_idx(v)
+        vlmin = float(np.log2(v[0]))
+        if idx is None:
+            dvl = max(float(np.log2(v[1]) - np.log2(v[0])), EPS64)
+            return 2. ** (vlmin + (np.floor((wl - vlmin) / dvl) + .5) * dvl)
+        vlmin1 = float(np.log2(v[idx - 1]))
+        dvl0 = max(float(np.log2(v[1]) - np.log2(v[0])), EPS64)
+        dvl1 = max(float(np.log2(v[idx]) - np.log2(v[idx - 1])), EPS64)
+        hi = 2. ** (vlmin1 + (np.floor((wl - vlmin1) / dvl1) + .5) * dvl1)
+        lo = 2. ** (vlmin + (np.floor((wl - vlmin) / dvl0) + .5) * dvl0)
+        edge = np.where(wl > vlmin1, hi, lo)
+        split = 2. ** vlmin1
+        return np.where(np.abs(w - split) < np.abs(w - edge), split, edge)
+
+
+def bin_parity(idx, Wx, dWx, ssq_freqs, logscale, flipud, gamma, no_bin=0xFFFF):
+    """Compare a bin index computed elsewhere (`idx`, (na, N) integers,
+    `no_bin` where |Wx| <= gamma) with the float64 bins of (Wx, dWx).
+
+    Returns a dict of counts: entries, mismatched bins among entries both
+    keep, of which `near_edge` have the float64 w within one float32 ulp of
+    the rounding edge between the two bins (ties that float32 data cannot
+    resolve), `other` the rest; mask disagreements, of which `near_gamma`
+    have |Wx| within 1e-12 of gamma (relative)."""
+    w = phase_cwt(Wx, dWx, gamma)
+    a = np.abs(Wx)
+    use = a > gamma
+    k = bin_index(np.where(use, w, 1.), ssq_freqs, logscale, flipud)
+    got = np.asarray(idx).astype(np.int64)
+    keep = got != no_bin
+    both = use & keep
+    mis = both & (got != k)
+    wm = w[mis]
+    ulp = np.spacing(wm.astype(np.float32)).astype(np.float64)
+    near = np.abs(wm - bin_edge_w(wm, ssq_freqs, logscale)) <= ulp
+    mask_mis = use != keep
+    near_g = np.abs(a[mask_mis] - gamma) <= 1e-12 * gamma
+    return dict(entries=int(use.size), kept=int(use.sum()), mismatched=int(mis.sum()),
+                near_edge=int(near.sum()), other=int((~near).sum()),
+                mask_mismatched=int(mask_mis.sum()), mask_near_gamma=int(near_g.sum()),
+                mask_other=int((~near_g).sum()))
+
+
 def squeeze(Wx, k, use, const):
     """Tx[k[i,j], j] += Wx[i,j]*const[i] over i ascending, for `use` entries.
 

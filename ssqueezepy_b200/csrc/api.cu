@@ -542,11 +542,14 @@ int ssqb_cwt_noalloc(const void* x, int B, int N, int Npad, int n1, int padtype,
                      const ssqb_wavelet* wavelet, double dt, const ssqb_bins* bins,
                      double gamma, int precision, void* Wx, void* dWx, void* w,
                      uint16_t* idx, int idx_pitch, void* stream) {
-  if (B < 1 || na < 1 || !is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
-    return ssqb_cwt(x, B, N, Npad, n1, padtype, rpadded, scales, na, wavelet, dt, bins,
-                    gamma, precision, Wx, dWx, w, idx, idx_pitch, nullptr, 0, stream);
+  // the checks that size the scratch come first, with ssqb_cwt's codes and
+  // messages; ssqb_cwt repeats all of its checks on the call below
+  if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
   if (!valid_precision(precision))
     return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
+    return fail(SSQB_EUNSUPPORTED, "Npad must be a power of two in [8, 2^22]");
+  if (B > 65535 || na > 65535) return fail(SSQB_EINVAL, "B and na must be <= 65535");
   const size_t need = xhat_bytes(B, Npad) + min_z_bytes(B, Npad, precision);
   if (need > kNoAllocScratchBytes)
     return fail(SSQB_EINVAL,
@@ -673,12 +676,15 @@ int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_sig* sigs
   const size_t smem = (size_t)max_na * 8 * sizeof(float2) + (size_t)max_na * sizeof(float);
   if (smem > 227 * 1024)
     return fail(SSQB_EUNSUPPORTED, "too many bins for the shared-memory squeeze");
+  bool aligned = true;
+  for (int i = 0; i < nsig; ++i)
+    aligned = aligned && sigs[i].idx_pitch % 32 == 0 && sigs[i].idx_off % 8 == 0;
   Tables tb;
   r = get_tables(&tb);
   if (r) return r;
   int e = run_squeeze_batch_f32((const float2*)Wx, idx,
                                 reinterpret_cast<const SigDesc*>(sigs_dev), nsig, max_na,
-                                max_N, (float2*)Tx, tb.status, (cudaStream_t)stream);
+                                max_N, aligned, (float2*)Tx, tb.status, (cudaStream_t)stream);
   if (e) return cuda_fail((cudaError_t)e, "squeeze launch");
   return SSQB_OK;
 }

@@ -218,3 +218,36 @@ def test_batch_autotune_picks_a_budget_and_keeps_results():
         for (t, w, _, _), (t0, w0) in zip(outs, ref):
             assert torch.equal(t, t0) and torch.equal(w, w0)
     assert L.device_status() == 0
+
+
+@pytest.mark.gpu
+def test_full_uneven_batch_every_signal_against_oracle():
+    """The batched workload itself: 256 chirp mixtures with lengths uniform in
+    [4096, 65536] (seed 1234), Morlet mu=6, one plan replayed as a CUDA graph.
+    Every signal's Tx and Wx against the float64 oracle (the oracle runs the
+    signals in parallel threads); max and median are printed."""
+    torch = _gpu()
+    from concurrent.futures import ThreadPoolExecutor
+    from ssqueezepy_b200._batch import SsqCwtBatch
+    from oracle import ssq_oracle as O
+    from tests._cases import rel_l2
+    xs = [x.astype(np.float32) for x in S.uneven_batch(256, 4096, 65536, 1234)]
+    plan = SsqCwtBatch([len(x) for x in xs], wavelet=('morlet', {'mu': 6.}), graph=True)
+    outs = plan(xs)
+    torch.cuda.synchronize()
+
+    def one(i):
+        t, w, f, _ = outs[i]
+        Tx, Wx = t.cpu().numpy(), w.cpu().numpy()
+        To, Wo, _ = O.ssq_cwt(xs[i].astype(np.float64), 'morlet', (6.,), plan.scales64[i],
+                              f[::-1].copy(), plan.weights64[i], gamma=10 * O.EPS32)
+        return rel_l2(Wx, Wo), rel_l2(Tx, To)
+
+    with ThreadPoolExecutor(4) as ex:
+        errs = np.array(list(ex.map(one, range(len(xs)))))
+    print(f'\n256 signals: Wx rel-L2 max {errs[:, 0].max():.2e} median '
+          f'{np.median(errs[:, 0]):.2e}; Tx rel-L2 max {errs[:, 1].max():.2e} '
+          f'median {np.median(errs[:, 1]):.2e}')
+    assert errs[:, 0].max() <= 1e-5
+    assert errs[:, 1].max() <= 1e-4
+    assert L.device_status() == 0

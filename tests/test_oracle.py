@@ -184,3 +184,43 @@ def test_oracle_ridges_match_golden():
                 assert np.array_equal(i, g[key + '_idx']), key
                 assert np.array_equal(f, g[key + '_f']), key
                 assert np.allclose(e, g[key + '_e'], rtol=1e-6 if dt == 'f32' else 1e-14), key
+
+
+def test_bin_parity_counts_and_edges():
+    """The bin-parity checker: the oracle's own bins give no mismatch; a
+    moved bin counts as `other`; an entry whose w sits at its rounding edge,
+    given the bin across the edge, counts as `near_edge`."""
+    from ssqueezepy_b200 import _transforms as T
+    from tests._cases import chirp_signal
+    N = 2000
+    x = chirp_signal(N).astype(np.float32).astype(np.float64)
+    wav = P.Wavelet(('morlet', {'mu': 6.}))
+    s = P.process_scales('log-piecewise', N, wav, nv=32).ravel()
+    fp = T._ssq_plan(wav, 'log-piecewise', N, 32, None, 'peak', 'reflect', 1.)
+    W, dW = O.cwt(x, 'morlet', (6.,), s)
+    g = 10 * P.EPS32
+    w = O.phase_cwt(W, dW, g)
+    use = np.abs(W) > g
+    k = np.where(use, O.bin_index(np.where(use, w, 1.), fp['f_asc'], True, True), 0xFFFF)
+    r = O.bin_parity(k, W, dW, fp['f_asc'], True, True, g)
+    assert r['mismatched'] == 0 and r['mask_mismatched'] == 0
+    i, j = np.argwhere(use)[100]
+    k2 = k.copy()
+    k2[i, j] = (k2[i, j] + 3) % len(s)
+    r = O.bin_parity(k2, W, dW, fp['f_asc'], True, True, g)
+    assert r['mismatched'] == 1 and r['other'] == 1
+    # every entry's edge lies within half a bin of it
+    e = O.bin_edge_w(w[use], fp['f_asc'], True)
+    ratio = np.log2(e / w[use]) / np.log2(fp['f_asc'][1] / fp['f_asc'][0])
+    assert np.all(np.abs(ratio) <= 0.5 + 1e-9)
+    ei = O.bin_edge_w(np.array([w[i, j]]), fp['f_asc'], True)[0]
+    dW2 = dW.copy()
+    dW2[i, j] *= ei / w[i, j]
+    w2 = O.phase_cwt(W, dW2, g)[i, j]
+    kk = O.bin_index(np.array([w2]), fp['f_asc'], True, True)[0]
+    res = []
+    for d in (-1, 1):
+        k3 = k.copy()
+        k3[i, j] = kk + d
+        res.append(O.bin_parity(k3, W, dW2, fp['f_asc'], True, True, g))
+    assert any(r['near_edge'] == 1 and r['other'] == 0 for r in res), res
