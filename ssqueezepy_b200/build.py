@@ -38,6 +38,20 @@ def _deps():
     return files
 
 
+def _includes(src, seen=None):
+    """`src` and the files it includes with quoted #include, recursively."""
+    import re
+    seen = set() if seen is None else seen
+    src = os.path.abspath(src)
+    if src in seen or not os.path.exists(src):
+        return seen
+    seen.add(src)
+    with open(src) as f:
+        for m in re.finditer(r'^\s*#include\s+"([^"]+)"', f.read(), re.M):
+            _includes(os.path.join(os.path.dirname(src), m.group(1)), seen)
+    return seen
+
+
 def up_to_date():
     if not os.path.exists(LIB):
         return False
@@ -52,15 +66,14 @@ def build(force=False, jobs=None, verbose=False):
     os.makedirs(OBJDIR, exist_ok=True)
     srcs = _sources()
 
-    # an object is reused when it is newer than its source and than every
-    # shared header (and this script); otherwise it is rebuilt
-    shared = [f for f in _deps() if not f.endswith('.cu')]
-    t_shared = max(os.path.getmtime(f) for f in shared)
-
+    # an object is reused when it is newer than its source, than every
+    # header it includes (followed through quoted #include lines) and than
+    # this script; otherwise it is rebuilt
     def compile_one(src):
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + '.o')
+        t_dep = max(os.path.getmtime(f) for f in _includes(src))
         if (not force and os.path.exists(obj)
-                and os.path.getmtime(obj) >= max(os.path.getmtime(src), t_shared)):
+                and os.path.getmtime(obj) >= max(t_dep, os.path.getmtime(__file__))):
             return obj
         cmd = [NVCC, *ARCH, *FLAGS, '-I', INCLUDE, '-c', src, '-o', obj]
         if verbose:

@@ -37,17 +37,18 @@ static int launch_sq(const C* Wx, const Src& src, const double* cst, int B, int 
 template <typename C>
 static bool cols_ok(const void* idx, int idx_pitch, int na, int nbins) {
   return SSQB_SQ_COLS && idx_pitch % 32 == 0 && ((uintptr_t)idx & 15) == 0 &&
-         squeeze_cols_smem<C>(na, nbins) <= 227 * 1024;
+         squeeze_tile_smem<C>(na, nbins) <= 227 * 1024;
 }
 
 template <typename C>
 static int launch_sq_cols(const C* Wx, const uint16_t* idx, int idx_pitch, const double* cst,
                           int B, int na, int N, int nbins, C* Tx, int* status,
                           cudaStream_t st) {
-  const size_t smem = squeeze_cols_smem<C>(na, nbins);
+  const size_t smem = squeeze_tile_smem<C>(na, nbins);
   auto k = squeeze_cols_kernel<C>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
+  if (!e) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e) return e;
   dim3 grid((N + 31) / 32, B);
   k<<<grid, 32, smem, st>>>(Wx, idx, idx_pitch, cst, na, N, nbins, Tx, status);
@@ -85,10 +86,11 @@ int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* 
                           int* status, cudaStream_t st) {
   if (int* c = launch_counter()) return ++*c, 0;
   if (aligned && cols_ok<float2>(idx, 32, max_na, max_na)) {
-    const size_t smem = squeeze_cols_smem<float2>(max_na, max_na);
+    const size_t smem = squeeze_tile_smem<float2>(max_na, max_na);
     auto k = squeeze_cols_batch_kernel<float2>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
+    if (!e) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e) return e;
     dim3 grid((max_N + 31) / 32, nsig);
     k<<<grid, 32, smem, st>>>(Wx, idx, desc, Tx, status);
