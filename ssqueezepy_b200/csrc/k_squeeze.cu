@@ -32,7 +32,7 @@ static int launch_sq(const C* Wx, const Src& src, const double* cst, int B, int 
 // multiple of 32 columns, 16-byte aligned index) and its accumulator fits
 // shared memory; else the row-group kernel above.
 #ifndef SSQB_SQ_COLS
-#define SSQB_SQ_COLS 1
+#define SSQB_SQ_COLS 0
 #endif
 template <typename C>
 static bool cols_ok(const void* idx, int idx_pitch, int na, int nbins) {

@@ -35,7 +35,7 @@ template <typename C> __host__ __device__ constexpr int tile_of() {
 // Pass 1 of split-load ops forms its inputs in shared memory first (1) or
 // gathers them per butterfly item (0).
 #ifndef SSQB_P1_STAGE
-#define SSQB_P1_STAGE 1
+#define SSQB_P1_STAGE 0
 #endif
 template <typename C> struct MinBlocks { static constexpr int v = 2; };
 template <> struct MinBlocks<double2> { static constexpr int v = SSQB_FP64_MINBLOCKS; };

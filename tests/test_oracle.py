@@ -224,3 +224,25 @@ def test_bin_parity_counts_and_edges():
         k3[i, j] = kk + d
         res.append(O.bin_parity(k3, W, dW2, fp['f_asc'], True, True, g))
     assert any(r['near_edge'] == 1 and r['other'] == 0 for r in res), res
+
+
+def test_cpu_path_port_tracks_float64_oracle():
+    """The timed CPU arm (the reference's float32 CPU execution): Wx at the
+    float32 level of the float64 oracle, Tx at the reference's own float32
+    level (bin flips of entries near an edge, ~1e-3)."""
+    from oracle.ssq_cpu_path import SsqCwtCpu
+    from ssqueezepy_b200 import _transforms as T
+    from tests._cases import chirp_signal, rel_l2
+    N = 3000
+    x = chirp_signal(N).astype(np.float32)
+    wav = P.Wavelet(('gmw', {'gamma': 3., 'beta': 60.}))
+    s = P.process_scales('log-piecewise', N, wav, nv=32).ravel()
+    fp = T._ssq_plan(wav, 'log-piecewise', N, 32, None, 'peak', 'reflect', 1.)
+    port = SsqCwtCpu(N, 'gmw_l1', (3., 60.), s, fp['mode'], fp['bp'], fp['const'])
+    Tx, Wx = port(x)
+    To, Wo, _ = O.ssq_cwt(x.astype(np.float64), 'gmw_l1', (3., 60.), s, fp['f_asc'],
+                          fp['const'], gamma=10 * O.EPS32)
+    assert rel_l2(Wx, Wo) < 1e-5
+    assert rel_l2(Tx, To) < 1e-2
+    Tx2, _ = port(x)
+    assert np.array_equal(Tx, Tx2)  # deterministic: columns are independent
