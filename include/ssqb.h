@@ -125,6 +125,23 @@ SSQB_API int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype
              void* Wx, void* dWx, void* w, uint16_t* idx, int idx_pitch,
              void* workspace, size_t workspace_bytes, void* stream);
 
+/* ssqb_cwt with the scale values also given on the host (`scales_host`, na
+ * doubles equal to the device `scales`; NULL makes it ssqb_cwt). They let
+ * the call plan per row: rows whose wavelet band spans at most a quarter of
+ * a transform tile (512 bins with float64 arithmetic, 1024 with SSQB_F32) go
+ * through a band-limited single pass (D = Npad / M transforms of the
+ * twiddled band, M the band's power-of-two length, no two-pass
+ * intermediate) instead of the four-step of the full padded length. Same
+ * outputs, workspace and stream semantics as ssqb_cwt. No reference
+ * counterpart (the reference multiplies the full padded spectrum and takes
+ * full-length inverse FFTs of every row, _cwt.py:167-177). */
+SSQB_API int ssqb_cwt_ex(const void* x, int B, int N, int Npad, int n1, int padtype,
+                         int rpadded, const double* scales, const double* scales_host,
+                         int na, const ssqb_wavelet* wavelet, double dt,
+                         const ssqb_bins* bins, double gamma, int precision, void* Wx,
+                         void* dWx, void* w, uint16_t* idx, int idx_pitch, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
 /* Squeeze from a bin index: Tx[b, idx, j] += Wx[b, i, j] * row_weights[i]
  * over i ascending (algos.py:859-984 accumulation order). idx rows have
  * idx_pitch columns (0 = N). Tx (B, nbins, N) is overwritten. */

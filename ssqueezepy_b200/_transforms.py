@@ -198,10 +198,11 @@ def _cwt_core(x, wavelet, scales, nv, fs, t, padtype, rpadded, nan_checks,
     cw = L.wavelet_struct(kernel or wavelet)
     cb = L.make_bins(*ssq) if ssq is not None else None
     gamma = _default_gamma(dtype) if gamma is None else gamma
+    sc_h = np.ascontiguousarray(scales_np, np.float64)  # lets the call plan per row
     with torch.cuda.device(dev):
-        rc = L.load().ssqb_cwt(
+        rc = L.load().ssqb_cwt_ex(
             L.ptr(xd), B, N, Npad, n1, ptype, 1 if (rpadded and padtype) else 0,
-            L.ptr(sc_d), na, cw, float(dt), cb, float(gamma), prec,
+            L.ptr(sc_d), sc_h.ctypes.data, na, cw, float(dt), cb, float(gamma), prec,
             L.ptr(Wx), L.ptr(dWx), L.ptr(w), L.ptr(idx), ipitch, L.ptr(ws), wsb,
             L.stream_ptr())
     L.check(rc, 'cwt')

@@ -5,6 +5,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 #include "launch.h"
 #include "../../include/ssqb.h"
 
@@ -202,6 +203,48 @@ static int check_sigs(const ssqb_sig* s, int nsig, int Npad, bool need_scales,
   return SSQB_OK;
 }
 
+// Rows whose wavelet band fits at most 2^max_log bins, as band_bins
+// evaluates it on the device (the same float64 expressions): the longest
+// suffix of such rows, in groups of equal band length, takes the
+// band-limited single pass. No host scales: every row takes the tile passes.
+static void cwt_band_plan(const double* sc, int na, int Npad, const WavDev& wd, int max_log,
+                          BandPlan* bp) {
+  bp->two_pass_rows = na;
+  bp->ngroups = 0;
+  if (!sc || !(wd.lo < wd.hi)) return;
+  const double h = (2 * M_PI) / Npad;
+  std::vector<int> lg(na);
+  for (int i = 0; i < na; ++i) {
+    const double sh = sc[i] * h;
+    const double a = std::floor(wd.lo / sh) - 1.0, c = std::ceil(wd.hi / sh) + 1.0;
+    const int klo = (int)std::fmax(std::fmin(a, (double)Npad), -(double)Npad);
+    const int khi = (int)std::fmax(std::fmin(c, (double)Npad), -(double)Npad);
+    int l = 3;
+    while ((1 << l) < khi - klo + 1) ++l;
+    lg[i] = l;
+  }
+  int s = na;
+  while (s > 0 && lg[s - 1] <= max_log) --s;
+  if (s == na) return;
+  bp->two_pass_rows = s;
+  for (int i = s; i < na;) {
+    int j = i;
+    while (j < na && lg[j] == lg[i]) ++j;
+    int g = bp->ngroups;
+    if (g == BandPlan::kMaxGroups) {  // fold the rest into the last group
+      g -= 1;
+      bp->nrows[g] += j - i;
+      if (lg[i] > bp->logM[g]) bp->logM[g] = lg[i];
+    } else {
+      bp->r0[g] = i;
+      bp->nrows[g] = j - i;
+      bp->logM[g] = lg[i];
+      bp->ngroups = g + 1;
+    }
+    i = j;
+  }
+}
+
 }  // namespace ssqb
 
 using namespace ssqb;
@@ -278,11 +321,12 @@ int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_b
   return count;
 }
 
-int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
-             const double* scales, int na, const ssqb_wavelet* wavelet, double dt,
-             const ssqb_bins* bins, double gamma, int precision,
-             void* Wx, void* dWx, void* w, uint16_t* idx, int idx_pitch,
-             void* workspace, size_t workspace_bytes, void* stream) {
+static int cwt_impl(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
+                    const double* scales, int na, const ssqb_wavelet* wavelet, double dt,
+                    const ssqb_bins* bins, double gamma, int precision,
+                    void* Wx, void* dWx, void* w, uint16_t* idx, int idx_pitch,
+                    void* workspace, size_t workspace_bytes, void* stream,
+                    const double* scales_host) {
   if (!x || !scales || !Wx || !workspace) return fail(SSQB_EINVAL, "NULL pointer argument");
   if (B < 1 || N < 1 || na < 1) return fail(SSQB_EINVAL, "B, N and na must be >= 1");
   if (!valid_precision(precision))
@@ -326,24 +370,48 @@ int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpa
   const int m = ilog2i(Npad);
   const double h = (2 * M_PI) / Npad;
   const int oN = rpadded ? Npad : N, on1 = rpadded ? 0 : n1;
+  BandPlan bp{};
+  const int max_log =
+      ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE : FftCfg<double2>::TILE) - 2;
+  cwt_band_plan(scales_host, na, Npad, wd, max_log, &bp);
   if (precision == SSQB_F32) {
     CwtOp<float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,
                      (float)(1.0 / Npad), gamma, (float2*)Wx, (float2*)dWx, (float*)w,
                      idx, idx_pitch, tb.status};
-    e = run_cwt_f32(op, B, m, (float2*)zb, zbytes / sizeof(float2), tb, st);
+    e = run_cwt_f32(op, B, m, (float2*)zb, zbytes / sizeof(float2), tb, st, &bp);
   } else if (precision == SSQB_F32X) {
     CwtOp<double2, float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,
                               1.0 / Npad, gamma, (float2*)Wx, (float2*)dWx, (float*)w,
                               idx, idx_pitch, tb.status};
-    e = run_cwt_f32x(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st);
+    e = run_cwt_f32x(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st, &bp);
   } else {
     CwtOp<double2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt, 1.0 / Npad,
                       gamma, (double2*)Wx, (double2*)dWx, (double*)w, idx, idx_pitch,
                       tb.status};
-    e = run_cwt_f64(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st);
+    e = run_cwt_f64(op, B, m, (double2*)zb, zbytes / sizeof(double2), tb, st, &bp);
   }
   if (e) return cuda_fail((cudaError_t)e, "cwt launch");
   return SSQB_OK;
+}
+
+int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
+             const double* scales, int na, const ssqb_wavelet* wavelet, double dt,
+             const ssqb_bins* bins, double gamma, int precision,
+             void* Wx, void* dWx, void* w, uint16_t* idx, int idx_pitch,
+             void* workspace, size_t workspace_bytes, void* stream) {
+  return cwt_impl(x, B, N, Npad, n1, padtype, rpadded, scales, na, wavelet, dt, bins, gamma,
+                  precision, Wx, dWx, w, idx, idx_pitch, workspace, workspace_bytes, stream,
+                  nullptr);
+}
+
+int ssqb_cwt_ex(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
+                const double* scales, const double* scales_host, int na,
+                const ssqb_wavelet* wavelet, double dt, const ssqb_bins* bins, double gamma,
+                int precision, void* Wx, void* dWx, void* w, uint16_t* idx, int idx_pitch,
+                void* workspace, size_t workspace_bytes, void* stream) {
+  return cwt_impl(x, B, N, Npad, n1, padtype, rpadded, scales, na, wavelet, dt, bins, gamma,
+                  precision, Wx, dWx, w, idx, idx_pitch, workspace, workspace_bytes, stream,
+                  scales_host);
 }
 
 static int squeeze_common(const void* Wx, int kind, const void* src, int idx_pitch,

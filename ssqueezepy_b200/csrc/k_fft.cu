@@ -46,20 +46,39 @@ int run_xhat_f64(const double* x, int B, int N, int Npad, int n1, int padtype,
   return run_tile<XhatOp<double>, double2, -1>(op, B, 1, ilog2(Npad), Z, zcap, tb, st);
 }
 
+// tile passes for rows [0, two_pass_rows), then each band group
+template <class Op, typename C>
+static int run_cwt_t(const Op& op, int B, int log2L, C* Z, size_t zcap, const Tables& tb,
+                     cudaStream_t st, const BandPlan* bp) {
+  if (!bp || bp->ngroups == 0 || !two_pass<C>(log2L))
+    return run_tile_signals<Op, C, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
+  if (bp->two_pass_rows > 0) {
+    Op o = op;
+    o.nrun = bp->two_pass_rows;
+    const int e = run_tile_signals<Op, C, 1>(o, B, o.nrun, log2L, Z, zcap, tb, st);
+    if (e) return e;
+  }
+  for (int g = 0; g < bp->ngroups; ++g) {
+    const int e = run_band<Op, C, 1>(op, B, log2L, bp->logM[g], Z, zcap, bp->r0[g],
+                                     bp->nrows[g], tb, st);
+    if (e) return e;
+  }
+  return 0;
+}
+
 int run_cwt_f32(const CwtOp<float2>& op, int B, int log2L, float2* Z, size_t zcap,
-                const Tables& tb, cudaStream_t st) {
-  return run_tile_signals<CwtOp<float2>, float2, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
+                const Tables& tb, cudaStream_t st, const BandPlan* bp) {
+  return run_cwt_t(op, B, log2L, Z, zcap, tb, st, bp);
 }
 
 int run_cwt_f64(const CwtOp<double2>& op, int B, int log2L, double2* Z, size_t zcap,
-                const Tables& tb, cudaStream_t st) {
-  return run_tile_signals<CwtOp<double2>, double2, 1>(op, B, op.na, log2L, Z, zcap, tb, st);
+                const Tables& tb, cudaStream_t st, const BandPlan* bp) {
+  return run_cwt_t(op, B, log2L, Z, zcap, tb, st, bp);
 }
 
 int run_cwt_f32x(const CwtOp<double2, float2>& op, int B, int log2L, double2* Z,
-                 size_t zcap, const Tables& tb, cudaStream_t st) {
-  return run_tile_signals<CwtOp<double2, float2>, double2, 1>(op, B, op.na, log2L, Z, zcap,
-                                                               tb, st);
+                 size_t zcap, const Tables& tb, cudaStream_t st, const BandPlan* bp) {
+  return run_cwt_t(op, B, log2L, Z, zcap, tb, st, bp);
 }
 
 // trigdiff: rows in chunks of `chunk` through the spectrum buffer xh

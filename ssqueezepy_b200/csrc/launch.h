@@ -65,12 +65,23 @@ int run_xhat_f32(const float* x, int B, int N, int Npad, int n1, int padtype,
 int run_xhat_f64(const double* x, int B, int N, int Npad, int n1, int padtype,
                  double2* xh, double2* Z, size_t zcap, const Tables& tb,
                  cudaStream_t st);
+// Rows of a CWT call whose wavelet band fits M = 2^logM bins (a suffix of
+// the rows, in groups of one M each) take the band-limited single pass; rows
+// [0, two_pass_rows) take the tile passes. Built on the host from the scale
+// values (cwt_band_plan); without it every row takes the tile passes.
+struct BandPlan {
+  static constexpr int kMaxGroups = 16;
+  int two_pass_rows;
+  int ngroups;
+  int r0[kMaxGroups], nrows[kMaxGroups], logM[kMaxGroups];
+};
 int run_cwt_f32(const CwtOp<float2>& op, int B, int log2L, float2* Z, size_t zcap,
-                const Tables& tb, cudaStream_t st);
+                const Tables& tb, cudaStream_t st, const BandPlan* bp = nullptr);
 int run_cwt_f64(const CwtOp<double2>& op, int B, int log2L, double2* Z, size_t zcap,
-                const Tables& tb, cudaStream_t st);
+                const Tables& tb, cudaStream_t st, const BandPlan* bp = nullptr);
 int run_cwt_f32x(const CwtOp<double2, float2>& op, int B, int log2L, double2* Z,
-                 size_t zcap, const Tables& tb, cudaStream_t st);
+                 size_t zcap, const Tables& tb, cudaStream_t st,
+                 const BandPlan* bp = nullptr);
 int run_istft_frames_any_f32(const float2* Sx, int B, int L, int nframes, float* gu,
                              const Tables& tb, cudaStream_t st);
 int run_istft_frames_any_f64(const double2* Sx, int B, int L, int nframes, double* gu,

@@ -350,8 +350,10 @@ struct CwtOp {
   uint16_t* idx;          // optional bin index, (B, na, idx_pitch)
   int idx_pitch;
   int* status;
+  int nrun = 0;           // rows the tile passes run (0: all na); the rest go
+                          // through the band-limited single pass
   __device__ CwtOp bind(int) const { return *this; }
-  __device__ int rows() const { return na; }
+  __device__ int rows() const { return nrun > 0 ? nrun : na; }
   // the same op for signals b0, b0+1, ... (pointers advanced by b0 signals)
   __host__ __device__ CwtOp shifted(int b0) const {
     CwtOp o = *this;

@@ -323,6 +323,137 @@ tile_pass2(Op op, Tables tb, const C* __restrict__ Z, int log2L, int row_lo,
   fft_rows<C, LOGL1, NF, kNT, SIGN, NARR, MAP_J, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
 
+// ---- band-limited single pass ---------------------------------------------------
+// A row whose wavelet band (signed bins [klo, khi], op.band_bins) fits in M
+// bins needs no four-step. With D = L / M and n = D a + n2 (n2 < D, a < M),
+//   y[D a + n2] = e^{SIGN 2 pi i klo n / L}
+//                 sum_{m<M} (Zb[m] e^{SIGN 2 pi i m n2 / L}) e^{SIGN 2 pi i m a / M},
+// Zb[m] = the transform's input at bin klo + m (zero past khi): D transforms of
+// length M of the twiddled band. A CTA takes NF = TILE / M consecutive
+// residues n2, so each output index a gives NF consecutive columns.
+//
+// band_prep: Zb[(b, r)][a][m] for rows row0 + r (both arrays), the band's
+// inputs formed once per row (spectrum x wavelet in float64, as pass 1).
+template <class Op, typename C>
+__global__ void __launch_bounds__(kNT)
+band_prep(Op op, C* __restrict__ Zb, int row0, int nrows, int logM) {
+  constexpr int NARR = Op::NARR;
+  const auto bop = op.bind(blockIdx.z);
+  const int b = Op::kBatch ? 0 : blockIdx.z;
+  const int row = row0 + blockIdx.x;
+  const int M = 1 << logM;
+  int klo, khi;
+  bop.band_bins(row, klo, khi);
+  C* zb = Zb + ((size_t)blockIdx.z * nrows + blockIdx.x) * NARR * M;
+  if (khi - klo + 1 > M && threadIdx.x == 0) set_status(bop.status, DEV_BAD_INDEX);
+  for (int m = threadIdx.x; m < M; m += kNT) {
+    const int kk = klo + m;
+    C v[NARR];
+    if (kk <= khi) {
+      const int k = kk < 0 ? kk + bop.Npad : kk;
+      bop.apply(k, bop.raw(b, k, klo, khi), bop.psi(row, k), v);
+    } else {
+#pragma unroll
+      for (int a = 0; a < NARR; ++a)
+        v[a] = mk((typename RealOf<C>::type)0, (typename RealOf<C>::type)0);
+    }
+#pragma unroll
+    for (int a = 0; a < NARR; ++a) zb[a * M + m] = v[a];
+  }
+}
+
+// first-stage gather of the twiddled band: inputs j + r*stride of residue
+// n2_0 + f, twiddles by recurrence from two table values
+template <typename C, int NARR, int SIGN>
+struct BandLoader {
+  static constexpr bool kGather = true;
+  const Tables& tb;
+  const C* zb;
+  int M, n2_0, log2L;
+  __device__ __forceinline__ void operator()(int f, int m, C (&v)[NARR]) const {
+    const uint64_t mask = ((uint64_t)1 << log2L) - 1;
+    const C w = to_c<C>(unit_root<SIGN>(tb, (uint32_t)(((uint64_t)m * (n2_0 + f)) & mask),
+                                        log2L));
+#pragma unroll
+    for (int a = 0; a < NARR; ++a) v[a] = cmul(__ldg(zb + a * M + m), w);
+  }
+  template <int R>
+  __device__ __forceinline__ void gather(int f, int j, int stride, C (&t)[R][NARR]) const {
+    const uint64_t mask = ((uint64_t)1 << log2L) - 1;
+    const uint64_t n2 = (uint64_t)(n2_0 + f);
+    C raw[R][NARR];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int a = 0; a < NARR; ++a) raw[r][a] = __ldg(zb + a * M + j + r * stride);
+    double2 w = unit_root<SIGN>(tb, (uint32_t)(((uint64_t)j * n2) & mask), log2L);
+    const double2 s = unit_root<SIGN>(tb, (uint32_t)(((uint64_t)stride * n2) & mask), log2L);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const C wc = to_c<C>(w);
+#pragma unroll
+      for (int a = 0; a < NARR; ++a) t[r][a] = cmul(raw[r][a], wc);
+      w = mk(w.x * s.x - w.y * s.y, w.x * s.y + w.y * s.x);
+    }
+  }
+};
+
+// storer: output a = m0 + r*stride of residue n2_0 + f is column
+// n = D a + n2_0 + f, times e^{SIGN 2 pi i klo n / L}, handed to op.store
+template <class BOp, typename C, int SIGN>
+struct BandStore {
+  static constexpr int NARR = BOp::NARR;
+  const BOp& op;
+  const Tables& tb;
+  int b, row, D, n2_0, klo, log2L;
+  template <int R>
+  __device__ __forceinline__ void item(int f, int m0, int stride, C (&a)[R], C (&z)[R]) const {
+    const int64_t L = (int64_t)1 << log2L;
+    const int n0 = D * m0 + n2_0 + f;      // column of r = 0
+    const int64_t kl = ((int64_t)klo % L + L) % L;
+    double2 p = unit_root<SIGN>(tb, (uint32_t)((kl * n0) & (L - 1)), log2L);
+    const double2 s = unit_root<SIGN>(tb, (uint32_t)((kl * D * stride) & (L - 1)), log2L);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const C pc = to_c<C>(p);
+      C v[NARR];
+      v[0] = cmul(a[r], pc);
+      v[NARR - 1] = cmul(z[r], pc);
+      op.store(b, row, n0 + D * stride * r, v);
+      p = mk(p.x * s.x - p.y * s.y, p.x * s.y + p.y * s.x);
+    }
+  }
+};
+
+// CTA = (NF residues, row row0 + blockIdx.y, batch item)
+template <class Op, typename C, int LOGM, int SIGN>
+__global__ void __launch_bounds__(kNT, MinBlocks<C>::v)
+band_single(Op op, Tables tb, const C* __restrict__ Zb, int log2L, int row0, int nrows) {
+  constexpr int NARR = Op::NARR;
+  constexpr int TILE = tile_of<C>();
+  constexpr int M = 1 << LOGM;
+  constexpr int NF = TILE / M;
+  typedef Layout<C, LOGM, NF> LY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* base = reinterpret_cast<C*>(smem_raw);
+  C* bufs[NARR];
+#pragma unroll
+  for (int a = 0; a < NARR; ++a) bufs[a] = base + a * LY::ARR;
+  C* const(&buf)[NARR] = bufs;
+  const auto bop = op.bind(blockIdx.z);
+  const int b = Op::kBatch ? 0 : blockIdx.z;
+  const int row = row0 + blockIdx.y;
+  int klo, khi;
+  bop.band_bins(row, klo, khi);
+  const C* zb = Zb + ((size_t)blockIdx.z * nrows + blockIdx.y) * NARR * M;
+  const int n2_0 = blockIdx.x * NF;
+  const int D = 1 << (log2L - LOGM);
+  BandLoader<C, NARR, SIGN> ld{tb, zb, M, n2_0, log2L};
+  typedef decltype(op.bind(0)) BOp;
+  BandStore<BOp, C, SIGN> st{bop, tb, b, row, D, n2_0, klo, log2L};
+  fft_rows<C, LOGM, NF, kNT, SIGN, NARR, MAP_J, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
+}
+
 // shared memory of one tile kernel: NARR arrays of NF rows at the row pitch
 template <typename C>
 inline size_t tile_smem(int narr, int logl) {

@@ -163,6 +163,55 @@ static int run_batch(BOp op, int nsig, int nrows, int log2L, C* Z, size_t zcap,
   return 0;
 }
 
+// Band-limited single pass over rows [r0, r0 + nrows) whose bands fit M =
+// 2^logM bins: per chunk of signals (their band inputs Zb fit the
+// intermediate), band_prep then band_single.
+template <class Op, typename C, int SIGN, int LOGM>
+static int launch_band(const Op& op, int B, int log2L, C* Z, int r0, int nrows,
+                       const Tables& tb, cudaStream_t st) {
+  if (int* c = launch_counter()) return *c += 2, 0;
+  constexpr int NF = tile_of<C>() / (1 << LOGM);
+  band_prep<Op, C><<<dim3(nrows, 1, B), kNT, 0, st>>>(op, Z, r0, nrows, LOGM);
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
+  const size_t smem = tile_smem<C>(Op::NARR, LOGM);
+  auto k = band_single<Op, C, LOGM, SIGN>;
+  e = prep(k, smem);
+  if (e) return e;
+  dim3 grid((1u << (log2L - LOGM)) / NF, nrows, B);
+  k<<<grid, kNT, smem, st>>>(op, tb, Z, log2L, r0, nrows);
+  return cudaGetLastError();
+}
+
+template <typename C> constexpr int band_max_log() { return tile_log<C>() - 2; }
+
+template <class Op, typename C, int SIGN>
+static int run_band(const Op& op, int B, int log2L, int logM, C* Z, size_t zcap, int r0,
+                    int nrows, const Tables& tb, cudaStream_t st) {
+  const size_t per = (size_t)Op::NARR << logM;  // one signal-row of band inputs
+  const size_t rc = zcap / per;                  // signal-rows that fit
+  if (rc < 1) return (int)cudaErrorInvalidValue;
+  int nb = 1, rstep = nrows;
+  if ((size_t)nrows <= rc) {
+    const size_t q = rc / nrows;
+    nb = q < (size_t)B ? (int)q : B;
+  } else {
+    rstep = (int)rc;
+  }
+  for (int b0 = 0; b0 < B; b0 += nb) {
+    const int n = B - b0 < nb ? B - b0 : nb;
+    for (int q0 = 0; q0 < nrows; q0 += rstep) {
+      const int nr = nrows - q0 < rstep ? nrows - q0 : rstep;
+      const int e = dispatch_log<3, band_max_log<C>()>(logM, [&](auto k) {
+        return launch_band<Op, C, SIGN, decltype(k)::value>(op.shifted(b0), n, log2L, Z,
+                                                            r0 + q0, nr, tb, st);
+      });
+      if (e) return e;
+    }
+  }
+  return 0;
+}
+
 // Signals of one call in chunks when all of them need more than half of the
 // intermediate per row: each chunk's row fits half of the L2 budget, so its
 // row tiles alternate between two streams (ops with `shifted(b0)`).
