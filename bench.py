@@ -256,14 +256,15 @@ def run_ours(args):
     prec = L.F32X if args.arith == 'float64' else L.F32
     wsb = max(wsb, lib.ssqb_cwt_workspace_bytes(1, N, Npad, na, prec))
     ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
-    launches = lib.ssqb_cwt_launches(1, Npad, na, prec, wsb) + 1
+    sc_h = np.ascontiguousarray(sc, np.float64)  # host scales: per-row plan
+    launches = lib.ssqb_cwt_ex_launches(1, Npad, na, prec, wsb, sc_h.ctypes.data, cw) + 1
 
     def step(ev=None, prec=prec):
         if ev:
             ev[0].record(st)
-        L.check(lib.ssqb_cwt(L.ptr(x), 1, N, Npad, n1, 1, 0, L.ptr(sc_d), na, cw, 1.0,
-                             cb, gamma, prec, L.ptr(Wx), None, None, L.ptr(idx),
-                             ipitch, L.ptr(ws), wsb, sp), 'cwt')
+        L.check(lib.ssqb_cwt_ex(L.ptr(x), 1, N, Npad, n1, 1, 0, L.ptr(sc_d),
+                                sc_h.ctypes.data, na, cw, 1.0, cb, gamma, prec, L.ptr(Wx),
+                                None, None, L.ptr(idx), ipitch, L.ptr(ws), wsb, sp), 'cwt')
         if ev:
             ev[1].record(st)
         L.check(lib.ssqb_squeeze(L.ptr(Wx), L.ptr(idx), ipitch, L.ptr(cst_d), 1, na, N,

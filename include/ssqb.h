@@ -142,6 +142,12 @@ SSQB_API int ssqb_cwt_ex(const void* x, int B, int N, int Npad, int n1, int padt
                          void* dWx, void* w, uint16_t* idx, int idx_pitch, void* workspace,
                          size_t workspace_bytes, void* stream);
 
+/* Number of kernel launches one ssqb_cwt_ex call makes with these host
+ * scales and this workspace size; no reference counterpart. */
+SSQB_API int ssqb_cwt_ex_launches(int B, int Npad, int na, int precision,
+                                  size_t workspace_bytes, const double* scales_host,
+                                  const ssqb_wavelet* wavelet);
+
 /* Squeeze from a bin index: Tx[b, idx, j] += Wx[b, i, j] * row_weights[i]
  * over i ascending (algos.py:859-984 accumulation order). idx rows have
  * idx_pitch columns (0 = N). Tx (B, nbins, N) is overwritten. */

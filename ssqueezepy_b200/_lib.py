@@ -45,6 +45,7 @@ SIGNATURES = {
     'ssqb_cwt_ex': (_i, [_vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _i,
                          ctypes.POINTER(CWavelet), _d, ctypes.POINTER(CBins), _d, _i,
                          _vp, _vp, _vp, _vp, _i, _vp, _sz, _vp]),
+    'ssqb_cwt_ex_launches': (_i, [_i, _i, _i, _i, _sz, _vp, ctypes.POINTER(CWavelet)]),
     'ssqb_squeeze': (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _i, _i, _vp, _vp]),
     'ssqb_ssqueeze_fast': (_i, [_vp, _vp, _vp, _vp, ctypes.POINTER(CBins), _d,
                                 _i, _i, _i, _i, _vp, _vp]),

@@ -203,10 +203,16 @@ static int check_sigs(const ssqb_sig* s, int nsig, int Npad, bool need_scales,
   return SSQB_OK;
 }
 
+// band rows: bands of at most TILE / 2^SSQB_BAND_OFF bins, i.e.
+// 2^SSQB_BAND_OFF residues per CTA of the single pass (512 bins with float64
+// arithmetic measured faster than 256 or 1024 at N = 10,000 and 160,000)
+#ifndef SSQB_BAND_OFF
+#define SSQB_BAND_OFF 2
+#endif
 // Rows whose wavelet band fits at most 2^max_log bins, as band_bins
 // evaluates it on the device (the same float64 expressions): the longest
-// suffix of such rows, in groups of equal band length, takes the
-// band-limited single pass. No host scales: every row takes the tile passes.
+// suffix of such rows takes the band-limited single pass. No host scales:
+// every row takes the tile passes.
 static void cwt_band_plan(const double* sc, int na, int Npad, const WavDev& wd, int max_log,
                           BandPlan* bp) {
   bp->two_pass_rows = na;
@@ -226,23 +232,16 @@ static void cwt_band_plan(const double* sc, int na, int Npad, const WavDev& wd, 
   int s = na;
   while (s > 0 && lg[s - 1] <= max_log) --s;
   if (s == na) return;
+  // one group at the largest band length of the suffix: two launches in all
+  // (per-length groups measured slower, their launches cost more than the
+  // narrower transforms save)
   bp->two_pass_rows = s;
-  for (int i = s; i < na;) {
-    int j = i;
-    while (j < na && lg[j] == lg[i]) ++j;
-    int g = bp->ngroups;
-    if (g == BandPlan::kMaxGroups) {  // fold the rest into the last group
-      g -= 1;
-      bp->nrows[g] += j - i;
-      if (lg[i] > bp->logM[g]) bp->logM[g] = lg[i];
-    } else {
-      bp->r0[g] = i;
-      bp->nrows[g] = j - i;
-      bp->logM[g] = lg[i];
-      bp->ngroups = g + 1;
-    }
-    i = j;
-  }
+  bp->ngroups = 1;
+  bp->r0[0] = s;
+  bp->nrows[0] = na - s;
+  bp->logM[0] = 3;
+  for (int i = s; i < na; ++i)
+    if (lg[i] > bp->logM[0]) bp->logM[0] = lg[i];
 }
 
 }  // namespace ssqb
@@ -293,7 +292,8 @@ size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
   return xhat_bytes(B, Npad) + z;
 }
 
-int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_bytes) {
+static int cwt_launches_impl(int B, int Npad, int na, int precision, size_t workspace_bytes,
+                             const BandPlan* bp) {
   if (B < 1 || na < 1 || !is_pow2(Npad) || Npad < 8 || Npad > (1 << 22)) return -1;
   if (!valid_precision(precision)) return -1;
   const size_t xb = xhat_bytes(B, Npad);
@@ -307,18 +307,33 @@ int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_b
   if (precision == SSQB_F32) {
     CwtOp<float2> op{};
     op.na = na;
-    run_cwt_f32(op, B, m, nullptr, zbytes / sizeof(float2), tb, 0);
+    run_cwt_f32(op, B, m, nullptr, zbytes / sizeof(float2), tb, 0, bp);
   } else if (precision == SSQB_F32X) {
     CwtOp<double2, float2> op{};
     op.na = na;
-    run_cwt_f32x(op, B, m, nullptr, zbytes / sizeof(double2), tb, 0);
+    run_cwt_f32x(op, B, m, nullptr, zbytes / sizeof(double2), tb, 0, bp);
   } else {
     CwtOp<double2> op{};
     op.na = na;
-    run_cwt_f64(op, B, m, nullptr, zbytes / sizeof(double2), tb, 0);
+    run_cwt_f64(op, B, m, nullptr, zbytes / sizeof(double2), tb, 0, bp);
   }
   set_launch_counter(nullptr);
   return count;
+}
+
+int ssqb_cwt_launches(int B, int Npad, int na, int precision, size_t workspace_bytes) {
+  return cwt_launches_impl(B, Npad, na, precision, workspace_bytes, nullptr);
+}
+
+int ssqb_cwt_ex_launches(int B, int Npad, int na, int precision, size_t workspace_bytes,
+                         const double* scales_host, const ssqb_wavelet* wavelet) {
+  WavDev wd;
+  if (!scales_host || check_wavelet(wavelet, &wd)) return -1;
+  BandPlan bp{};
+  const int max_log = ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE
+                                                  : FftCfg<double2>::TILE) - SSQB_BAND_OFF;
+  cwt_band_plan(scales_host, na, Npad, wd, max_log, &bp);
+  return cwt_launches_impl(B, Npad, na, precision, workspace_bytes, &bp);
 }
 
 static int cwt_impl(const void* x, int B, int N, int Npad, int n1, int padtype, int rpadded,
@@ -371,8 +386,8 @@ static int cwt_impl(const void* x, int B, int N, int Npad, int n1, int padtype, 
   const double h = (2 * M_PI) / Npad;
   const int oN = rpadded ? Npad : N, on1 = rpadded ? 0 : n1;
   BandPlan bp{};
-  const int max_log =
-      ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE : FftCfg<double2>::TILE) - 2;
+  const int max_log = ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE
+                                                  : FftCfg<double2>::TILE) - SSQB_BAND_OFF;
   cwt_band_plan(scales_host, na, Npad, wd, max_log, &bp);
   if (precision == SSQB_F32) {
     CwtOp<float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,

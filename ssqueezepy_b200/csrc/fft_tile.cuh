@@ -177,7 +177,7 @@ struct HasGather<T, std::void_t<decltype(T::kGather)>> : std::bool_constant<T::k
 template <typename C, int LOGL, int NF, int NT, int SIGN, int NARR, int MAP_IN, int MAP_OUT,
           bool DIRECT_OUT, int S, class LD, class ST>
 __device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __restrict__ seg,
-                                          const LD& ld, const ST& st) {
+                                          const LD& ld, const ST& st, int tid) {
   typedef Layout<C, LOGL, NF> LY;
   constexpr int RL_MAX = FftCfg<C>::RMAX_LOG;
   constexpr int NSTG = fft_nstages(LOGL, RL_MAX);
@@ -191,7 +191,6 @@ __device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __rest
   constexpr int PER = cdiv(NB, NT);
   constexpr bool FIRST = (S == 0), LAST = (S == NSTG - 1);
   constexpr int MAP = FIRST ? MAP_IN : (LAST ? MAP_OUT : MAP_J);
-  const int tid = threadIdx.x;
   C v[NARR][PER][R];
   // gather
 #pragma unroll
@@ -257,14 +256,18 @@ __device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __rest
   if constexpr (!(LAST && DIRECT_OUT)) __syncthreads();
   if constexpr (!LAST)
     fft_stage<C, LOGL, NF, NT, SIGN, NARR, MAP_IN, MAP_OUT, DIRECT_OUT, S + 1>(buf, seg, ld,
-                                                                             st);
+                                                                             st, tid);
 }
 
+// tid: this thread's index among the NT threads of the transform (a CTA can
+// run several transforms side by side, each with its own NT threads; the
+// stage barriers are CTA-wide, so all of them take the same stages)
 template <typename C, int LOGL, int NF, int NT, int SIGN, int NARR, int MAP_IN, int MAP_OUT,
           bool DIRECT_OUT, class LD, class ST>
 __device__ __forceinline__ void fft_rows(C* const (&buf)[NARR], const C* __restrict__ seg,
-                                         const LD& ld, const ST& st) {
-  fft_stage<C, LOGL, NF, NT, SIGN, NARR, MAP_IN, MAP_OUT, DIRECT_OUT, 0>(buf, seg, ld, st);
+                                         const LD& ld, const ST& st, int tid = threadIdx.x) {
+  fft_stage<C, LOGL, NF, NT, SIGN, NARR, MAP_IN, MAP_OUT, DIRECT_OUT, 0>(buf, seg, ld, st,
+                                                                         tid);
 }
 
 }  // namespace ssqb

@@ -94,30 +94,34 @@ __device__ __forceinline__ int pad_src(long long q, int N, int padtype) {
 }
 
 // ---- wavelets, float64 (wavelets.py:521-527, _gmw.py:203-210, 246-251) --
-__device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
-  if (w.lo < w.hi && (x < w.lo || x > w.hi)) return 0.0;
-  if (w.kind == 0) {
-    // C1 (ea - ks ec), ea = exp(-(x-mu)^2/2), ec = exp(-x^2/2). The ratio of
-    // the two terms is ks ec / ea = exp(-mu x): where mu |x| >= 40 the
-    // smaller one is below 2^-57 of the larger, under a quarter ulp, and
-    // the difference rounds to the larger term alone, so its exp is skipped.
-    const double mx = w.p0 * x;
-    const double d = x - w.p0;
-    const double a = -0.5 * (d * d);
-    const double c = -0.5 * (x * x);
-    const double ea = (a > -708.0 && mx > -40.0) ? exp(a) : 0.0;
-    const double ec = (c > -708.0 && mx < 40.0) ? exp(c) : 0.0;
-    return w.p2 * (ea - w.p1 * ec);
-  }
-  if (x <= 0.0) return 0.0;
-  if (w.kind == 1 && w.ibeta >= 0 && w.p0 == 3.0) {
-    // 2 exp(beta ln(x/wc) - (x^3 - wc^3)) = 2 (x/wc)^beta exp(wc^3 - x^3)
-    const double x3 = x * x * x;
-    const double e = w.wcg - x3;
-    if (!(e > -708.0)) return 0.0;
-    const double f = w.npoly ? gmw_poly(w, x3) : 2.0;
-    return f * powi(x / w.p2, w.ibeta) * exp(e);
-  }
+// Formula branches; psih_fp64 picks one per call, the fused CWT's loads pick
+// one per item (psih_kind), so the code a kind runs stays contiguous.
+__device__ __forceinline__ double psih_morlet(const WavDev& w, double x) {
+  // C1 (ea - ks ec), ea = exp(-(x-mu)^2/2), ec = exp(-x^2/2). The ratio of
+  // the two terms is ks ec / ea = exp(-mu x): where mu |x| >= 40 the
+  // smaller one is below 2^-57 of the larger, under a quarter ulp, and
+  // the difference rounds to the larger term alone, so its exp is skipped.
+  const double mx = w.p0 * x;
+  const double d = x - w.p0;
+  const double a = -0.5 * (d * d);
+  const double c = -0.5 * (x * x);
+  const double ea = (a > -708.0 && mx > -40.0) ? exp(a) : 0.0;
+  const double ec = (c > -708.0 && mx < 40.0) ? exp(c) : 0.0;
+  return w.p2 * (ea - w.p1 * ec);
+}
+
+// GMW L1 with gamma = 3 and an integer beta: 2 exp(beta ln(x/wc) - (x^3 -
+// wc^3)) = 2 (x/wc)^beta exp(wc^3 - x^3), x > 0
+__device__ __forceinline__ double psih_gmw3(const WavDev& w, double x) {
+  const double x3 = x * x * x;
+  const double e = w.wcg - x3;
+  if (!(e > -708.0)) return 0.0;
+  const double f = w.npoly ? gmw_poly(w, x3) : 2.0;
+  return f * powi(x / w.p2, w.ibeta) * exp(e);
+}
+
+// GMW L1 / L2, any gamma and beta, x > 0
+__device__ __forceinline__ double psih_gmw(const WavDev& w, double x) {
   const double lw = log(x);
   const double xg = (w.p0 == 3.0) ? x * x * x : exp(w.p0 * lw);
   if (w.kind == 1) {
@@ -129,6 +133,31 @@ __device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
   const double e = w.p1 * lw - xg;
   if (!(e > -708.0)) return 0.0;
   return (w.npoly ? gmw_poly(w, xg) : w.p3) * exp(e);
+}
+
+// 0 Morlet, 1 GMW L1 gamma 3 integer beta, 2 other GMW
+__device__ __forceinline__ int psih_kind_of(const WavDev& w) {
+  if (w.kind == 0) return 0;
+  return (w.kind == 1 && w.ibeta >= 0 && w.p0 == 3.0) ? 1 : 2;
+}
+
+template <int KIND>
+__device__ __forceinline__ double psih_kind(const WavDev& w, double x) {
+  if (w.lo < w.hi && (x < w.lo || x > w.hi)) return 0.0;
+  if constexpr (KIND == 0) {
+    return psih_morlet(w, x);
+  } else {
+    if (x <= 0.0) return 0.0;
+    if constexpr (KIND == 1) return psih_gmw3(w, x);
+    else return psih_gmw(w, x);
+  }
+}
+
+__device__ __forceinline__ double psih_fp64(const WavDev& w, double x) {
+  const int k = psih_kind_of(w);
+  if (k == 0) return psih_kind<0>(w, x);
+  if (k == 1) return psih_kind<1>(w, x);
+  return psih_kind<2>(w, x);
 }
 
 // ---- frequency bin (algos.py:859-953; round = half-to-even, as numba) ----
@@ -397,6 +426,15 @@ struct CwtOp {
     double ps = psih_fp64(wav, scales[row] * xi);
     if (k == (Npad >> 1)) ps *= 0.5;
     return ps;
+  }
+  // the same with the formula branch fixed (psih_kind_of(wav) == KIND)
+  template <int KIND>
+  __device__ __forceinline__ void finish_k(int row, int k, double2 xv, C (&v)[2]) const {
+    const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
+    const double xi = (double)kk * h;
+    double ps = psih_kind<KIND>(wav, scales[row] * xi);
+    if (k == (Npad >> 1)) ps *= 0.5;
+    apply(k, xv, ps, v);
   }
   __device__ void apply(int k, double2 xv, double ps, C (&v)[2]) const {
     const int kk = (k <= (Npad >> 1)) ? k : k - Npad;

@@ -33,10 +33,10 @@ static int launch_p1(const Op& op, int B, int log2L, C* Z, int row_lo, int rows,
                      const Tables& tb, cudaStream_t st) {
   if (int* c = launch_counter()) return ++*c, 0;
   const size_t smem = tile_smem<C>(Op::NARR, LOGL2);
+  dim3 grid((1u << log2L) / tile_of<C>(), rows, B);
   auto k = tile_pass1<Op, C, LOGL2, SIGN>;
   cudaError_t e = prep(k, smem);
   if (e) return e;
-  dim3 grid((1u << log2L) / tile_of<C>(), rows, B);
   k<<<grid, kNT, smem, st>>>(op, tb, Z, log2L, row_lo, rows);
   return cudaGetLastError();
 }
@@ -46,10 +46,10 @@ static int launch_p2(const Op& op, int B, int log2L, const C* Z, int row_lo, int
                      const Tables& tb, cudaStream_t st) {
   if (int* c = launch_counter()) return ++*c, 0;
   const size_t smem = tile_smem<C>(Op::NARR, LOGL1);
+  dim3 grid((1u << log2L) / tile_of<C>(), rows, B);
   auto k = tile_pass2<Op, C, LOGL1, SIGN>;
   cudaError_t e = prep(k, smem);
   if (e) return e;
-  dim3 grid((1u << log2L) / tile_of<C>(), rows, B);
   k<<<grid, kNT, smem, st>>>(op, tb, Z, log2L, row_lo, rows);
   return cudaGetLastError();
 }
@@ -175,15 +175,15 @@ static int launch_band(const Op& op, int B, int log2L, C* Z, int r0, int nrows,
   cudaError_t e = cudaGetLastError();
   if (e) return e;
   const size_t smem = tile_smem<C>(Op::NARR, LOGM);
+  dim3 grid((1u << (log2L - LOGM)) / NF, nrows, B);
   auto k = band_single<Op, C, LOGM, SIGN>;
   e = prep(k, smem);
   if (e) return e;
-  dim3 grid((1u << (log2L - LOGM)) / NF, nrows, B);
   k<<<grid, kNT, smem, st>>>(op, tb, Z, log2L, r0, nrows);
   return cudaGetLastError();
 }
 
-template <typename C> constexpr int band_max_log() { return tile_log<C>() - 2; }
+template <typename C> constexpr int band_max_log() { return tile_log<C>() - 1; }
 
 template <class Op, typename C, int SIGN>
 static int run_band(const Op& op, int B, int log2L, int logM, C* Z, size_t zcap, int r0,
