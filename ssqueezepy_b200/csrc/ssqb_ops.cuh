@@ -94,8 +94,7 @@ __device__ __forceinline__ int pad_src(long long q, int N, int padtype) {
 }
 
 // ---- wavelets, float64 (wavelets.py:521-527, _gmw.py:203-210, 246-251) --
-// Formula branches; psih_fp64 picks one per call, the fused CWT's loads pick
-// one per item (psih_kind), so the code a kind runs stays contiguous.
+// Formula branches; psih_fp64 picks one per call.
 __device__ __forceinline__ double psih_morlet(const WavDev& w, double x) {
   // C1 (ea - ks ec), ea = exp(-(x-mu)^2/2), ec = exp(-x^2/2). The ratio of
   // the two terms is ks ec / ea = exp(-mu x): where mu |x| >= 40 the
@@ -426,15 +425,6 @@ struct CwtOp {
     double ps = psih_fp64(wav, scales[row] * xi);
     if (k == (Npad >> 1)) ps *= 0.5;
     return ps;
-  }
-  // the same with the formula branch fixed (psih_kind_of(wav) == KIND)
-  template <int KIND>
-  __device__ __forceinline__ void finish_k(int row, int k, double2 xv, C (&v)[2]) const {
-    const int kk = (k <= (Npad >> 1)) ? k : k - Npad;
-    const double xi = (double)kk * h;
-    double ps = psih_kind<KIND>(wav, scales[row] * xi);
-    if (k == (Npad >> 1)) ps *= 0.5;
-    apply(k, xv, ps, v);
   }
   __device__ void apply(int k, double2 xv, double ps, C (&v)[2]) const {
     const int kk = (k <= (Npad >> 1)) ? k : k - Npad;

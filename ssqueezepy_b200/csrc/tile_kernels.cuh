@@ -147,22 +147,11 @@ struct P1Loader<BOp, C, NARR, std::enable_if_t<BOp::kSplitLoad>> {
         op.apply(k1_0 + f + L1 * (j + r * stride), raw[r], ps[r], t[r]);
     } else {
       // float64 transforms: all R evaluations inlined (loops unrolled 2 and 4
-      // measured 0.1 % and 1.5 % slower at N = 160,000), the wavelet's formula
-      // branch taken once for the item, so the code of one kind is contiguous
-      const int kind = psih_kind_of(op.wav);
-      if (kind == 0) {
+      // measured 0.1 % and 1.5 % slower at N = 160,000; the wavelet's formula
+      // branch hoisted out of the R evaluations, 2-4 % slower)
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-          op.template finish_k<0>(row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
-      } else if (kind == 1) {
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          op.template finish_k<1>(row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
-      } else {
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          op.template finish_k<2>(row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
-      }
+      for (int r = 0; r < R; ++r)
+        op.finish(b, row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
     }
   }
 };
