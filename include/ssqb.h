@@ -114,8 +114,7 @@ SSQB_API int ssqb_cwt_launches(int B, int Npad, int na, int precision,
  *   Wx     (B, na, N) complex, required; dWx optional (NULL)
  *   w      (B, na, N) real phase transform, optional (inf where |Wx|<gamma)
  *   idx    (B, na, idx_pitch) uint16 bin of each entry, 0xFFFF where
- *          |Wx|<=gamma; optional (needs `bins`); idx_pitch >= N columns (0 = N;
- *          a multiple of 32 lets ssqb_squeeze use its bulk-copy kernel)
+ *          |Wx|<=gamma; optional (needs `bins`); idx_pitch >= N columns (0 = N)
  * Npad is the padded length (a power of two, 8 <= Npad <= 2^22) and n1 the
  * left pad; dt = 1/fs. rpadded != 0 writes all Npad columns (outputs
  * (B, na, Npad), _cwt.py:293-306 with rpadded=True). */

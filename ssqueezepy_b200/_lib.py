@@ -181,8 +181,8 @@ def make_bins(mode, p, nbins, flipud):
 
 
 def idx_pitch(n):
-    """Row pitch of a bin-index buffer: n rounded up to 32 columns (lets the
-    squeeze stream rows with 16-byte bulk copies)."""
+    """Row pitch of a bin-index buffer: n rounded up to 32 columns (64-byte
+    aligned rows)."""
     return (n + 31) // 32 * 32
 
 

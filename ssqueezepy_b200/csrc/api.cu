@@ -759,15 +759,12 @@ int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_sig* sigs
   const size_t smem = (size_t)max_na * 8 * sizeof(float2) + (size_t)max_na * sizeof(float);
   if (smem > 227 * 1024)
     return fail(SSQB_EUNSUPPORTED, "too many bins for the shared-memory squeeze");
-  bool aligned = true;
-  for (int i = 0; i < nsig; ++i)
-    aligned = aligned && sigs[i].idx_pitch % 32 == 0 && sigs[i].idx_off % 8 == 0;
   Tables tb;
   r = get_tables(&tb);
   if (r) return r;
   int e = run_squeeze_batch_f32((const float2*)Wx, idx,
                                 reinterpret_cast<const SigDesc*>(sigs_dev), nsig, max_na,
-                                max_N, aligned, (float2*)Tx, tb.status, (cudaStream_t)stream);
+                                max_N, (float2*)Tx, tb.status, (cudaStream_t)stream);
   if (e) return cuda_fail((cudaError_t)e, "squeeze launch");
   return SSQB_OK;
 }

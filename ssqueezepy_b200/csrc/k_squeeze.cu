@@ -28,33 +28,6 @@ static int launch_sq(const C* Wx, const Src& src, const double* cst, int B, int 
   return cudaGetLastError();
 }
 
-// Column-tile squeeze from the bin index when its layout allows (pitch a
-// multiple of 32 columns, 16-byte aligned index) and its accumulator fits
-// shared memory; else the row-group kernel above.
-#ifndef SSQB_SQ_COLS
-#define SSQB_SQ_COLS 0
-#endif
-template <typename C>
-static bool cols_ok(const void* idx, int idx_pitch, int na, int nbins) {
-  return SSQB_SQ_COLS && idx_pitch % 32 == 0 && ((uintptr_t)idx & 15) == 0 &&
-         squeeze_tile_smem<C>(na, nbins) <= 227 * 1024;
-}
-
-template <typename C>
-static int launch_sq_cols(const C* Wx, const uint16_t* idx, int idx_pitch, const double* cst,
-                          int B, int na, int N, int nbins, C* Tx, int* status,
-                          cudaStream_t st) {
-  const size_t smem = squeeze_tile_smem<C>(na, nbins);
-  auto k = squeeze_cols_kernel<C>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (!e) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  if (e) return e;
-  dim3 grid((N + 31) / 32, B);
-  k<<<grid, 32, smem, st>>>(Wx, idx, idx_pitch, cst, na, N, nbins, Tx, status);
-  return cudaGetLastError();
-}
-
 template <typename C>
 static int run_sq(const C* Wx, int src_kind, const void* src, int idx_pitch,
                   const double* sfs, const BinDev& bins, double gamma, const double* cst,
@@ -62,9 +35,6 @@ static int run_sq(const C* Wx, int src_kind, const void* src, int idx_pitch,
   typedef typename RealOf<C>::type T;
   switch (src_kind) {
     case 0: {
-      if (cols_ok<C>(src, idx_pitch, na, nbins))
-        return launch_sq_cols(Wx, (const uint16_t*)src, idx_pitch, cst, B, na, N, nbins, Tx,
-                              status, st);
       IdxSrc<C> s{(const uint16_t*)src, idx_pitch, N};
       return launch_sq(Wx, s, cst, B, na, N, nbins, Tx, status, st);
     }
@@ -82,20 +52,9 @@ static int run_sq(const C* Wx, int src_kind, const void* src, int idx_pitch,
 }
 
 int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* desc,
-                          int nsig, int max_na, int max_N, bool aligned, float2* Tx,
-                          int* status, cudaStream_t st) {
+                          int nsig, int max_na, int max_N, float2* Tx, int* status,
+                          cudaStream_t st) {
   if (int* c = launch_counter()) return ++*c, 0;
-  if (aligned && cols_ok<float2>(idx, 32, max_na, max_na)) {
-    const size_t smem = squeeze_tile_smem<float2>(max_na, max_na);
-    auto k = squeeze_cols_batch_kernel<float2>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (!e) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e) return e;
-    dim3 grid((max_N + 31) / 32, nsig);
-    k<<<grid, 32, smem, st>>>(Wx, idx, desc, Tx, status);
-    return cudaGetLastError();
-  }
   constexpr int G = SSQB_SQ_G, U = SSQB_SQ_U, CW = 32 / G;
   const size_t smem = (size_t)max_na * CW * sizeof(float2) + (size_t)max_na * sizeof(float);
   auto k = squeeze_batch_kernel<float2, G, U>;

@@ -133,11 +133,9 @@ int run_cwt_batch_f32x(const CwtBatchOp<double2, float2>& op, int nsig, int max_
                        int log2L, double2* Z, size_t zcap, const Tables& tb, cudaStream_t st);
 int run_cwt_batch_f32(const CwtBatchOp<float2, float2>& op, int nsig, int max_na, int log2L,
                       float2* Z, size_t zcap, const Tables& tb, cudaStream_t st);
-// aligned: every signal's index pitch is a multiple of 32 columns and its
-// index offset a multiple of 8 entries (the column-tile kernel's copies)
 int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* desc,
-                          int nsig, int max_na, int max_N, bool aligned, float2* Tx,
-                          int* status, cudaStream_t st);
+                          int nsig, int max_na, int max_N, float2* Tx, int* status,
+                          cudaStream_t st);
 
 // ridge extraction (k_ridges.cu)
 size_t ridges_workspace(int nf, int N, bool f64);
