@@ -1,5 +1,6 @@
 // Fused STFT tile kernels (one pass; power-of-two n_fft up to one tile).
 #include "tile_launch.cuh"
+#include "fft_mixed.cuh"
 
 namespace ssqb {
 
@@ -155,12 +156,143 @@ static int launch_bluestein(const StftOp<TX, double2, OC>& op, int B, const Tabl
   return cudaGetLastError();
 }
 
+// The same chirp-z transform with a convolution length M = 3 * 2^k or 5 * 2^k
+// (mixed-radix Stockham, fft_mixed.cuh) where that is shorter than the power
+// of two: n_fft 598 convolves at 1280 instead of 2048. The twiddle table
+// W[m] = exp(2 pi i m / M) is filled once per (persistent) CTA.
+template <typename TX, typename OC, int M, class RL>
+__global__ void __launch_bounds__(kNT, kBluesteinCtas)
+stft_bluestein_mixed_kernel(StftOp<TX, double2, OC> op, Tables tb) {
+  typedef double2 C;
+  typedef typename RealOf<OC>::type OT;
+  constexpr int NF = tile_of<C>() / M;
+  typedef LayoutM<C, M, NF> LY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const bufA = reinterpret_cast<C*>(smem_raw);
+  C* const bufB = bufA + LY::ARR;
+  C* const bufC = bufA + 2 * LY::ARR;
+  C* const W = bufA + 3 * LY::ARR;
+  const int b = blockIdx.z;
+  const int L = op.L;
+  const C zero = make_double2(0.0, 0.0);
+  for (int m = threadIdx.x; m < M; m += kNT) {
+    double sv, cv;
+    sincospi((double)(2 * m) / (double)M, &sv, &cv);
+    W[m] = make_double2(cv, sv);
+  }
+  __syncthreads();
+  auto ldB = [&](int, int m, C (&v)[1]) {
+    v[0] = m < L ? chirp(m, L) : (m > M - L ? chirp(M - m, L) : zero);
+    v[0].y = -v[0].y;  // conj(c)
+  };
+  fft_mixed_rows<C, M, NF, kNT, -1, RL>(bufB, W, ldB);
+  const int ntile = (op.nframes + NF - 1) / NF;
+  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const int t0 = tile * NF;
+    auto ldA = [&](int f, int m, C (&v)[1]) {
+      const int t = t0 + f;
+      if (t >= op.nframes || m >= L) {
+        v[0] = zero;
+        return;
+      }
+      const int q = op.modulated ? (m + op.s21) % L : m;
+      const long long p = (long long)t * op.hop + q;
+      const int s = pad_src(p - op.n1, op.N, op.padtype);
+      const double xv = s >= 0 ? (double)op.x[(size_t)b * op.N + s] : 0.0;
+      const C z = make_double2(xv * __ldg(op.win + q), xv * __ldg(op.dwin + q));
+      v[0] = cmul(z, chirp(m, L));
+    };
+    fft_mixed_rows<C, M, NF, kNT, -1, RL>(bufA, W, ldA);
+    auto ldC = [&](int f, int m, C (&v)[1]) {
+      v[0] = cmul(bufA[LY::at(f, m)], bufB[LY::at(f, m)]);
+    };
+    fft_mixed_rows<C, M, NF, kNT, 1, RL>(bufC, W, ldC);
+    const int nrow = (L >> 1) + 1;
+    const double inv_m = 1.0 / M;
+    for (int e = threadIdx.x; e < NF * nrow; e += kNT) {
+      const int f = e % NF, n = e / NF;
+      const int t = t0 + f;
+      if (t >= op.nframes) continue;
+      const int nm = (L - n) % L;
+      C zk = cmul(bufC[LY::at(f, n)], chirp(n, L));
+      C zm = cmul(bufC[LY::at(f, nm)], chirp(nm, L));
+      zk.x *= inv_m; zk.y *= inv_m;
+      zm.x *= inv_m; zm.y *= inv_m;
+      const double hf = 0.5;
+      const C S = make_double2(hf * (zk.x + zm.x), hf * (zk.y - zm.y));
+      const C dS = make_double2(hf * (zk.y + zm.y), -hf * (zk.x - zm.x));
+      const size_t o = ((size_t)b * nrow + n) * op.nframes + t;
+      if (op.Sx) op.Sx[o] = out_c<OC>(S);
+      if (op.dSx) op.dSx[o] = out_c<OC>(dS);
+      if (op.idx) {
+        double wv;
+        const uint16_t k = phase_bin(S, dS, __ldg(op.sfs + n), true, op.bins, op.gamma,
+                                     op.status, op.w ? &wv : nullptr);
+        op.idx[((size_t)b * nrow + n) * op.idx_pitch + t] = k;
+        if (op.w) op.w[o] = (OT)wv;
+      } else if (op.w) {
+        op.w[o] = (OT)phase_w(S, dS, __ldg(op.sfs + n), true, op.gamma);
+      }
+    }
+    __syncthreads();  // bufC is rewritten by the next tile
+  }
+}
+
+template <typename TX, typename OC, int M, class RL>
+static int launch_bluestein_mixed(const StftOp<TX, double2, OC>& op, int B, const Tables& tb,
+                                  cudaStream_t st) {
+  constexpr int NF = tile_of<double2>() / M;
+  typedef LayoutM<double2, M, NF> LY;
+  const size_t smem = (3 * (size_t)LY::ARR + M) * sizeof(double2);
+  auto k = stft_bluestein_mixed_kernel<TX, OC, M, RL>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kNT, smem) != cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+    per_sm = 1;
+  }
+  const int ntile = (op.nframes + NF - 1) / NF;
+  int gx = sms * (per_sm > 0 ? per_sm : 1);
+  if (B > 1) gx = (gx + B - 1) / B;
+  if (gx > ntile) gx = ntile;
+  dim3 grid(gx, 1, B);
+  k<<<grid, kNT, smem, st>>>(op, tb);
+  return cudaGetLastError();
+}
+
+// Convolution length of the chirp-z transform of an n_fft of L: the smallest
+// of 2^k, 3 * 2^k (>= 192) and 5 * 2^k (>= 160) that is >= 2L - 1 and fits
+// the float64 tile.
+static int bluestein_length(int L) {
+  int best = 1 << 30;
+  for (int f : {1, 3, 5})
+    for (int m = f * 8; m <= tile_of<double2>(); m *= 2)
+      if (m >= 2 * L - 1 && m < best && (f == 1 || m >= 160)) best = m;
+  return best;
+}
+
 template <typename TX, typename OC>
 static int run_bluestein(const StftOp<TX, double2, OC>& op, int B, int log2M,
                          const Tables& tb, cudaStream_t st) {
-  return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
-    return launch_bluestein<TX, OC, decltype(k)::value>(op, B, tb, st);
-  });
+  switch (bluestein_length(op.L)) {
+    case 160: return launch_bluestein_mixed<TX, OC, 160, Radices<5, 8, 4>>(op, B, tb, st);
+    case 192: return launch_bluestein_mixed<TX, OC, 192, Radices<3, 8, 8>>(op, B, tb, st);
+    case 320: return launch_bluestein_mixed<TX, OC, 320, Radices<5, 8, 8>>(op, B, tb, st);
+    case 384: return launch_bluestein_mixed<TX, OC, 384, Radices<3, 8, 4, 4>>(op, B, tb, st);
+    case 640: return launch_bluestein_mixed<TX, OC, 640, Radices<5, 8, 4, 4>>(op, B, tb, st);
+    case 768: return launch_bluestein_mixed<TX, OC, 768, Radices<3, 8, 8, 4>>(op, B, tb, st);
+    case 1280: return launch_bluestein_mixed<TX, OC, 1280, Radices<5, 8, 8, 4>>(op, B, tb, st);
+    case 1536: return launch_bluestein_mixed<TX, OC, 1536, Radices<3, 8, 8, 8>>(op, B, tb, st);
+    default:
+      return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
+        return launch_bluestein<TX, OC, decltype(k)::value>(op, B, tb, st);
+      });
+  }
 }
 
 // ---- istft frames for any n_fft: the inverse real transform by chirp-z ------

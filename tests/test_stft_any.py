@@ -69,3 +69,22 @@ def test_default_n_fft_of_a_short_signal():
     assert Sx.shape[0] == 300 // 2 + 1
     Tx, *_ = sb.ssq_stft(x, dtype='float64')
     assert np.isfinite(Tx.cpu().numpy()).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('n_fft, M', [(80, 160), (90, 192), (300, 640), (700, 1536)])
+def test_stft_mixed_radix_lengths_match_oracle(n_fft, M):
+    """n_fft whose chirp-z convolution takes a mixed-radix length M (3 or 5
+    times a power of two, shorter than the power of two): Sx, dSx against the
+    float64 oracle, hop 1 and 3."""
+    sb = _gpu()
+    from oracle import ssq_oracle as O
+    from ssqueezepy_b200 import _params as P
+    x = np.random.default_rng(n_fft).standard_normal(2500)
+    win, dwin = P.get_window('hann', n_fft, n_fft, derivative=True)
+    for hop in (1, 3):
+        Sx, dSx = sb.stft(x, 'hann', n_fft=n_fft, hop_len=hop, derivative=True,
+                          dtype='float64')
+        So, dSo = O.stft(x, win, dwin, n_fft, hop=hop)
+        assert rel_l2(Sx.cpu().numpy(), So) <= 1e-11, (n_fft, M, hop)
+        assert rel_l2(dSx.cpu().numpy(), dSo) <= 1e-11, (n_fft, M, hop)
