@@ -121,7 +121,7 @@ __device__ __forceinline__ void fft_mixed_stage(C* __restrict__ buf, const C* __
         constexpr int step = M / (NS * R);
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          C w = W[(r * k * step) % M];
+          C w = W[r * k * step];  // r k < NS R, so the index stays below M
           if (SIGN < 0) w.y = -w.y;
           v[p][r] = cmul(v[p][r], w);
         }

@@ -160,8 +160,19 @@ static int launch_bluestein(const StftOp<TX, double2, OC>& op, int B, const Tabl
 // (mixed-radix Stockham, fft_mixed.cuh) where that is shorter than the power
 // of two: n_fft 598 convolves at 1280 instead of 2048. The twiddle table
 // W[m] = exp(2 pi i m / M) is filled once per (persistent) CTA.
+// threads of the mixed-radix kernel, and the radix schedule of 1280
+#ifndef SSQB_BLU_NT
+#define SSQB_BLU_NT 256
+#endif
+#ifndef SSQB_BLU_R1280
+#define SSQB_BLU_R1280 0
+#endif
+constexpr int kBluNT = SSQB_BLU_NT;
+typedef std::conditional_t<SSQB_BLU_R1280 == 0, Radices<5, 8, 8, 4>, Radices<5, 4, 4, 4, 4>>
+    Radices1280;
+
 template <typename TX, typename OC, int M, class RL>
-__global__ void __launch_bounds__(kNT, kBluesteinCtas)
+__global__ void __launch_bounds__(kBluNT, kBluesteinCtas)
 stft_bluestein_mixed_kernel(StftOp<TX, double2, OC> op, Tables tb) {
   typedef double2 C;
   typedef typename RealOf<OC>::type OT;
@@ -175,7 +186,7 @@ stft_bluestein_mixed_kernel(StftOp<TX, double2, OC> op, Tables tb) {
   const int b = blockIdx.z;
   const int L = op.L;
   const C zero = make_double2(0.0, 0.0);
-  for (int m = threadIdx.x; m < M; m += kNT) {
+  for (int m = threadIdx.x; m < M; m += kBluNT) {
     double sv, cv;
     sincospi((double)(2 * m) / (double)M, &sv, &cv);
     W[m] = make_double2(cv, sv);
@@ -185,7 +196,7 @@ stft_bluestein_mixed_kernel(StftOp<TX, double2, OC> op, Tables tb) {
     v[0] = m < L ? chirp(m, L) : (m > M - L ? chirp(M - m, L) : zero);
     v[0].y = -v[0].y;  // conj(c)
   };
-  fft_mixed_rows<C, M, NF, kNT, -1, RL>(bufB, W, ldB);
+  fft_mixed_rows<C, M, NF, kBluNT, -1, RL>(bufB, W, ldB);
   const int ntile = (op.nframes + NF - 1) / NF;
   for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
     const int t0 = tile * NF;
@@ -202,14 +213,14 @@ stft_bluestein_mixed_kernel(StftOp<TX, double2, OC> op, Tables tb) {
       const C z = make_double2(xv * __ldg(op.win + q), xv * __ldg(op.dwin + q));
       v[0] = cmul(z, chirp(m, L));
     };
-    fft_mixed_rows<C, M, NF, kNT, -1, RL>(bufA, W, ldA);
+    fft_mixed_rows<C, M, NF, kBluNT, -1, RL>(bufA, W, ldA);
     auto ldC = [&](int f, int m, C (&v)[1]) {
       v[0] = cmul(bufA[LY::at(f, m)], bufB[LY::at(f, m)]);
     };
-    fft_mixed_rows<C, M, NF, kNT, 1, RL>(bufC, W, ldC);
+    fft_mixed_rows<C, M, NF, kBluNT, 1, RL>(bufC, W, ldC);
     const int nrow = (L >> 1) + 1;
     const double inv_m = 1.0 / M;
-    for (int e = threadIdx.x; e < NF * nrow; e += kNT) {
+    for (int e = threadIdx.x; e < NF * nrow; e += kBluNT) {
       const int f = e % NF, n = e / NF;
       const int t = t0 + f;
       if (t >= op.nframes) continue;
@@ -251,7 +262,7 @@ static int launch_bluestein_mixed(const StftOp<TX, double2, OC>& op, int B, cons
   int dev = 0, sms = 148, per_sm = 1;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kNT, smem) != cudaSuccess) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kBluNT, smem) != cudaSuccess) {
     cudaGetLastError();
     sms = 148;
     per_sm = 1;
@@ -261,16 +272,20 @@ static int launch_bluestein_mixed(const StftOp<TX, double2, OC>& op, int B, cons
   if (B > 1) gx = (gx + B - 1) / B;
   if (gx > ntile) gx = ntile;
   dim3 grid(gx, 1, B);
-  k<<<grid, kNT, smem, st>>>(op, tb);
+  k<<<grid, kBluNT, smem, st>>>(op, tb);
   return cudaGetLastError();
 }
 
 // Convolution length of the chirp-z transform of an n_fft of L: the smallest
 // of 2^k, 3 * 2^k (>= 192) and 5 * 2^k (>= 160) that is >= 2L - 1 and fits
 // the float64 tile.
+#ifndef SSQB_BLU_MIXED
+#define SSQB_BLU_MIXED 1
+#endif
 static int bluestein_length(int L) {
   int best = 1 << 30;
   for (int f : {1, 3, 5})
+    if (f == 1 || SSQB_BLU_MIXED)
     for (int m = f * 8; m <= tile_of<double2>(); m *= 2)
       if (m >= 2 * L - 1 && m < best && (f == 1 || m >= 160)) best = m;
   return best;
@@ -286,7 +301,7 @@ static int run_bluestein(const StftOp<TX, double2, OC>& op, int B, int log2M,
     case 384: return launch_bluestein_mixed<TX, OC, 384, Radices<3, 8, 4, 4>>(op, B, tb, st);
     case 640: return launch_bluestein_mixed<TX, OC, 640, Radices<5, 8, 4, 4>>(op, B, tb, st);
     case 768: return launch_bluestein_mixed<TX, OC, 768, Radices<3, 8, 8, 4>>(op, B, tb, st);
-    case 1280: return launch_bluestein_mixed<TX, OC, 1280, Radices<5, 8, 8, 4>>(op, B, tb, st);
+    case 1280: return launch_bluestein_mixed<TX, OC, 1280, Radices1280>(op, B, tb, st);
     case 1536: return launch_bluestein_mixed<TX, OC, 1536, Radices<3, 8, 8, 8>>(op, B, tb, st);
     default:
       return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
