@@ -291,6 +291,34 @@ SSQB_API int ssqb_cwt_batch(const float* x, const ssqb_sig* sigs, const ssqb_sig
 SSQB_API int ssqb_cwt_batch_launches(const ssqb_sig* sigs, int nsig, int Npad, int precision,
                                      size_t workspace_bytes);
 
+/* ssqb_cwt_batch with rows band_from and on (of every signal that has them)
+ * through the band-limited single pass at 2^band_log bins (see ssqb_cwt_ex);
+ * every signal's rows from band_from must have wavelet bands of at most that
+ * many bins (ssqb_cwt_band_rows gives both figures for one signal's scales;
+ * a batch takes the largest band_from and band_log of its signals; a row
+ * found wider on the device sets the status word). band_from >= the largest
+ * na: ssqb_cwt_batch. No reference counterpart. */
+SSQB_API int ssqb_cwt_batch_ex(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_dev,
+                               int nsig, int Npad, int padtype, const ssqb_wavelet* wavelet,
+                               double dt, double gamma, int precision, void* Wx,
+                               uint16_t* idx, void* workspace, size_t workspace_bytes,
+                               int band_from, int band_log, void* stream);
+
+/* Launches of one ssqb_cwt_batch_ex call. */
+SSQB_API int ssqb_cwt_batch_ex_launches(const ssqb_sig* sigs, int nsig, int Npad,
+                                        int precision, size_t workspace_bytes, int band_from,
+                                        int band_log);
+
+/* The rows of a CWT with these host scales that ssqb_cwt_ex sends through the
+ * band-limited single pass: the first such row (`band_from`, na if none; the
+ * rest of the rows are such too) and the power of two of their largest band
+ * (`band_log`, 0 if none). max_bins: the largest band length allowed (a power
+ * of two of at most half a tile; 0 = the ssqb_cwt_ex default, 512 bins with
+ * float64 arithmetic). No reference counterpart. */
+SSQB_API int ssqb_cwt_band_rows(const double* scales_host, int na, int Npad,
+                                const ssqb_wavelet* wavelet, int precision, int max_bins,
+                                int* band_from, int* band_log);
+
 /* ssqb_squeeze over nsig signals of any lengths, one launch: Tx (complex64)
  * at each signal's out_offset, from its Wx block, idx block and weights. */
 SSQB_API int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_sig* sigs,

@@ -78,11 +78,15 @@ class SsqCwtBatch:
     call overwrites the previous call's outputs. `graph=True` captures the
     device work in a CUDA graph after one eager run and replays it.
     `autotune=True` picks, per padded-length group, the intermediate budget
-    (rows per tile and signals per chunk) that runs fastest on this device.
+    (rows per tile and signals per chunk) and the band bound (which rows take
+    the band-limited single pass) that run fastest on this device. Without
+    it, rows whose wavelet band fits 512 bins take the band pass.
     """
 
-    # intermediate budgets the autotuner tries per length group, bytes
-    TUNE_BUDGETS = (32 << 20, 64 << 20, 128 << 20, 256 << 20)
+    # intermediate budgets the autotuner tries per length group, bytes, and
+    # band bounds (bins; -1 = no band pass)
+    TUNE_BUDGETS = (64 << 20, 128 << 20, 256 << 20)
+    TUNE_BANDS = (-1, 256, 512, 1024)
 
     def __init__(self, lengths, wavelet='gmw', scales='log-piecewise', nv=32, fs=None,
                  padtype='reflect', maprange='peak', flipud=True, gamma=None,
@@ -133,14 +137,15 @@ class SsqCwtBatch:
             ws = max(ws, lib.ssqb_cwt_batch_workspace_bytes(len(sel), int(Npad),
                                                             self.prec))
         self.sig_dev = self._to_dev(sig)
-        for g in self.groups:  # the library's default budget per group
+        self.cw = L.wavelet_struct(wavelet)
+        for g in self.groups:  # the library's defaults per group
             g['ws'] = lib.ssqb_cwt_batch_workspace_bytes(g['n'], g['Npad'], self.prec)
+            g['band'] = self._band(g, 0)
         if autotune:
             xb = max(g['n'] * g['Npad'] * 16 for g in self.groups)
             ws = max(ws, xb + max(self.TUNE_BUDGETS))
         self.ws_bytes = ws
         self.ws = torch.empty(ws, dtype=torch.uint8, device=dev)
-        self.cw = L.wavelet_struct(wavelet)
         self.x = torch.empty(self.n_x, dtype=torch.float32, device=dev)
         self.Wx = torch.empty(self.n_out, dtype=torch.complex64, device=dev)
         self.Tx = torch.empty(self.n_out, dtype=torch.complex64, device=dev)
@@ -156,32 +161,56 @@ class SsqCwtBatch:
     def _to_dev(self, arr):
         return torch.as_tensor(arr.view(np.uint8).copy(), device=self.dev)
 
+    def _band(self, g, max_bins):
+        """(band_from, band_log) of a length group: the rows from which every
+        signal's wavelet bands fit 2^band_log <= max_bins bins (0: the
+        library's default bound; -1: no band pass), from the host scales."""
+        if max_bins < 0:
+            return 1 << 30, 0
+        lib = L.load()
+        bf_all, bl_all = 0, 0
+        bf, bl = ctypes.c_int(), ctypes.c_int()
+        for i in g['sel']:
+            sc = np.ascontiguousarray(self.scales64[i], np.float64)
+            rc = lib.ssqb_cwt_band_rows(sc.ctypes.data, len(sc), g['Npad'], self.cw,
+                                        self.prec, int(max_bins), ctypes.byref(bf),
+                                        ctypes.byref(bl))
+            L.check(rc, 'band_rows')
+            bf_all, bl_all = max(bf_all, bf.value), max(bl_all, bl.value)
+        na_max = int(max(len(self.scales64[i]) for i in g['sel']))
+        return (bf_all, bl_all) if bf_all < na_max and bl_all >= 3 else (1 << 30, 0)
+
     @property
     def launches(self):
         """Kernel launches of one run (all groups plus the squeeze)."""
         lib = L.load()
         n = 1
         for g in self.groups:
-            k = lib.ssqb_cwt_batch_launches(g['host'].ctypes.data_as(ctypes.c_void_p),
-                                            g['n'], g['Npad'], self.prec, g['ws'])
+            k = lib.ssqb_cwt_batch_ex_launches(g['host'].ctypes.data_as(ctypes.c_void_p),
+                                               g['n'], g['Npad'], self.prec, g['ws'],
+                                               *g['band'])
             if k < 0:
                 raise RuntimeError("launch count query failed")
             n += k
         return n
 
-    def _cwt_group(self, g, ws_bytes, st):
+    def _cwt_group(self, g, ws_bytes, st, band=None):
         lib = L.load()
-        rc = lib.ssqb_cwt_batch(
+        bf, bl = g['band'] if band is None else band
+        rc = lib.ssqb_cwt_batch_ex(
             L.ptr(self.x), g['host'].ctypes.data_as(ctypes.c_void_p), L.ptr(g['dev']),
             g['n'], g['Npad'], self.ptype, self.cw, float(self.dt), self.gamma, self.prec,
-            L.ptr(self.Wx), L.ptr(self.idx), L.ptr(self.ws), ws_bytes, st)
+            L.ptr(self.Wx), L.ptr(self.idx), L.ptr(self.ws), ws_bytes, bf, bl, st)
         L.check(rc, 'cwt_batch')
 
     def autotune(self, reps=2):
-        """Per length group, time the CWT under each intermediate budget of
-        TUNE_BUDGETS (which sets rows per tile and signals per chunk) with CUDA
-        events on the current stream, and keep the fastest. Runs on whatever
-        is in the packed input (the values do not change the work)."""
+        """Per length group, time the CWT over a small search space and keep
+        the fastest point: the intermediate budget (TUNE_BUDGETS: rows per
+        tile and signals per chunk) times the band bound (TUNE_BANDS: the
+        largest wavelet band, in bins, whose rows take the band-limited single
+        pass instead of the tile passes; -1 = none), with CUDA events on the
+        current stream. Runs on whatever is in the packed input (the values do
+        not change the work)."""
         st = torch.cuda.current_stream(self.dev)
         sp = L.stream_ptr(st)
         if not self._ran:  # a seeded stand-in signal until the first load
@@ -192,26 +221,33 @@ class SsqCwtBatch:
         for g in self.groups:
             xb = g['n'] * g['Npad'] * 16
             times = {}
+            bands = {mb: self._band(g, mb) for mb in self.TUNE_BANDS}
             for zb in self.TUNE_BUDGETS:
                 wsb = min(self.ws_bytes, xb + zb)
-                try:
-                    self._cwt_group(g, wsb, sp)  # warm (and too-small budgets refused)
-                except RuntimeError:
-                    continue
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(st)
-                for _ in range(reps):
-                    self._cwt_group(g, wsb, sp)
-                e1.record(st)
-                e1.synchronize()
-                times[wsb] = e0.elapsed_time(e1) / reps
-            best = min(times, key=times.get)
-            g['ws'] = best
-            self.tuning.append(dict(Npad=g['Npad'], signals=g['n'],
-                                    budget_mb=(best - xb) / 2**20,
-                                    ms={round((k - xb) / 2**20): round(v, 3)
-                                        for k, v in times.items()}))
+                for mb, band in bands.items():
+                    if mb >= 0 and band[0] >= (1 << 30):
+                        continue  # no band rows at this bound
+                    try:
+                        self._cwt_group(g, wsb, sp, band)  # warm; small budgets refused
+                    except RuntimeError:
+                        continue
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    for _ in range(reps):
+                        self._cwt_group(g, wsb, sp, band)
+                    e1.record(st)
+                    e1.synchronize()
+                    times[(wsb, mb)] = e0.elapsed_time(e1) / reps
+            (best_ws, best_mb) = min(times, key=times.get)
+            g['ws'], g['band'] = best_ws, bands[best_mb]
+            self.tuning.append(dict(
+                Npad=g['Npad'], signals=g['n'], budget_mb=(best_ws - xb) / 2**20,
+                band_bins=best_mb, band_from=bands[best_mb][0] if best_mb >= 0 else None,
+                ms={'%d MB/%s' % (round((k[0] - xb) / 2**20),
+                                  'off' if k[1] < 0 else ('%d bins' % k[1] if k[1] else
+                                                          'default')): round(v, 3)
+                    for k, v in times.items()}))
         self._graph = None
         return self.tuning
 

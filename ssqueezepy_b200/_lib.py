@@ -66,6 +66,11 @@ SIGNATURES = {
     'ssqb_cwt_batch': (_i, [_vp, _vp, _vp, _i, _i, _i, ctypes.POINTER(CWavelet), _d, _d,
                             _i, _vp, _vp, _vp, _sz, _vp]),
     'ssqb_cwt_batch_launches': (_i, [_vp, _i, _i, _i, _sz]),
+    'ssqb_cwt_batch_ex': (_i, [_vp, _vp, _vp, _i, _i, _i, ctypes.POINTER(CWavelet), _d, _d,
+                               _i, _vp, _vp, _vp, _sz, _i, _i, _vp]),
+    'ssqb_cwt_batch_ex_launches': (_i, [_vp, _i, _i, _i, _sz, _i, _i]),
+    'ssqb_cwt_band_rows': (_i, [_vp, _i, _i, ctypes.POINTER(CWavelet), _i, _i,
+                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     'ssqb_cwt_adjoint_workspace_bytes': (_sz, [_i, _i, _i, _i]),
     'ssqb_cwt_adjoint': (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _vp, _i, _i, _i, _i, _i,
                               _vp, _i, ctypes.POINTER(CWavelet), _i, _vp, _i, _vp, _sz,

@@ -671,10 +671,16 @@ size_t ssqb_cwt_batch_workspace_bytes(int nsig, int Npad, int precision) {
   return xhat_bytes(nsig, Npad) + batch_z_bytes(Npad, precision);
 }
 
-int ssqb_cwt_batch(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_dev, int nsig,
-                   int Npad, int padtype, const ssqb_wavelet* wavelet, double dt,
-                   double gamma, int precision, void* Wx, uint16_t* idx, void* workspace,
-                   size_t workspace_bytes, void* stream) {
+// band rows: at most half a tile of bins (at least two residues per CTA)
+static int band_log_max(int precision) {
+  return ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE : FftCfg<double2>::TILE) - 1;
+}
+
+static int cwt_batch_impl(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_dev,
+                          int nsig, int Npad, int padtype, const ssqb_wavelet* wavelet,
+                          double dt, double gamma, int precision, void* Wx, uint16_t* idx,
+                          void* workspace, size_t workspace_bytes, int band_from,
+                          int band_log, void* stream) {
   if (!x || !sigs_dev || !Wx || !idx || !workspace)
     return fail(SSQB_EINVAL, "NULL pointer argument");
   if (precision != SSQB_F32 && precision != SSQB_F32X)
@@ -689,6 +695,10 @@ int ssqb_cwt_batch(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_de
   WavDev wd;
   r = check_wavelet(wavelet, &wd);
   if (r) return r;
+  if (band_from < 0) return fail(SSQB_EINVAL, "band_from must be >= 0");
+  if (band_from < max_na && (band_log < 3 || band_log > band_log_max(precision)))
+    return fail(SSQB_EINVAL, "band_log must be in [3, " +
+                                 std::to_string(band_log_max(precision)) + "]");
   const size_t xb = xhat_bytes(nsig, Npad);
   const size_t need = xb + min_z_bytes(1, Npad, precision);
   if (workspace_bytes < need)
@@ -710,19 +720,64 @@ int ssqb_cwt_batch(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_de
   if (precision == SSQB_F32X) {
     CwtBatchOp<double2, float2> op{xh, dd, wd, Npad, h, 1.0 / dt, 1.0 / Npad, gamma,
                                    (float2*)Wx, idx, tb.status};
-    e = run_cwt_batch_f32x(op, nsig, max_na, m, (double2*)zb, zbytes / sizeof(double2), tb,
-                           st);
+    op.band_from = band_from;
+    e = run_cwt_batch_f32x(op, nsig, max_na, m, band_log, (double2*)zb,
+                           zbytes / sizeof(double2), tb, st);
   } else {
     CwtBatchOp<float2, float2> op{xh, dd, wd, Npad, h, 1.0 / dt, (float)(1.0 / Npad), gamma,
                                   (float2*)Wx, idx, tb.status};
-    e = run_cwt_batch_f32(op, nsig, max_na, m, (float2*)zb, zbytes / sizeof(float2), tb, st);
+    op.band_from = band_from;
+    e = run_cwt_batch_f32(op, nsig, max_na, m, band_log, (float2*)zb,
+                          zbytes / sizeof(float2), tb, st);
   }
   if (e) return cuda_fail((cudaError_t)e, "cwt launch");
   return SSQB_OK;
 }
 
-int ssqb_cwt_batch_launches(const ssqb_sig* sigs, int nsig, int Npad, int precision,
-                            size_t workspace_bytes) {
+int ssqb_cwt_batch(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_dev, int nsig,
+                   int Npad, int padtype, const ssqb_wavelet* wavelet, double dt,
+                   double gamma, int precision, void* Wx, uint16_t* idx, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  return cwt_batch_impl(x, sigs, sigs_dev, nsig, Npad, padtype, wavelet, dt, gamma,
+                        precision, Wx, idx, workspace, workspace_bytes, 0x7fffffff, 0, stream);
+}
+
+int ssqb_cwt_batch_ex(const float* x, const ssqb_sig* sigs, const ssqb_sig* sigs_dev,
+                      int nsig, int Npad, int padtype, const ssqb_wavelet* wavelet, double dt,
+                      double gamma, int precision, void* Wx, uint16_t* idx, void* workspace,
+                      size_t workspace_bytes, int band_from, int band_log, void* stream) {
+  return cwt_batch_impl(x, sigs, sigs_dev, nsig, Npad, padtype, wavelet, dt, gamma,
+                        precision, Wx, idx, workspace, workspace_bytes, band_from, band_log,
+                        stream);
+}
+
+int ssqb_cwt_band_rows(const double* scales_host, int na, int Npad,
+                       const ssqb_wavelet* wavelet, int precision, int max_bins,
+                       int* band_from, int* band_log) {
+  if (!scales_host || !band_from || !band_log) return fail(SSQB_EINVAL, "NULL pointer argument");
+  if (na < 1 || !is_pow2(Npad) || Npad < 8 || Npad > (1 << 22))
+    return fail(SSQB_EINVAL, "na must be >= 1 and Npad a power of two in [8, 2^22]");
+  if (!valid_precision(precision))
+    return fail(SSQB_EINVAL, "precision must be SSQB_F32, SSQB_F64 or SSQB_F32X");
+  WavDev wd;
+  int r = check_wavelet(wavelet, &wd);
+  if (r) return r;
+  int max_log = ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE
+                                             : FftCfg<double2>::TILE) - SSQB_BAND_OFF;
+  if (max_bins > 0) {
+    if (!is_pow2(max_bins) || ilog2i(max_bins) > band_log_max(precision))
+      return fail(SSQB_EINVAL, "max_bins must be a power of two of at most half a tile");
+    max_log = ilog2i(max_bins);
+  }
+  BandPlan bp{};
+  cwt_band_plan(scales_host, na, Npad, wd, max_log, &bp);
+  *band_from = bp.two_pass_rows;
+  *band_log = bp.ngroups ? bp.logM[0] : 0;
+  return SSQB_OK;
+}
+
+static int cwt_batch_launches_impl(const ssqb_sig* sigs, int nsig, int Npad, int precision,
+                                   size_t workspace_bytes, int band_from, int band_log) {
   if (precision != SSQB_F32 && precision != SSQB_F32X) return -1;
   if (!is_pow2(Npad) || Npad < 8 || Npad > (1 << 22)) return -1;
   int max_na = 0, max_N = 0;
@@ -738,13 +793,28 @@ int ssqb_cwt_batch_launches(const ssqb_sig* sigs, int nsig, int Npad, int precis
   const int m = ilog2i(Npad);
   if (precision == SSQB_F32X) {
     CwtBatchOp<double2, float2> op{};
-    run_cwt_batch_f32x(op, nsig, max_na, m, nullptr, zbytes / sizeof(double2), tb, 0);
+    op.band_from = band_from;
+    run_cwt_batch_f32x(op, nsig, max_na, m, band_log, nullptr, zbytes / sizeof(double2), tb,
+                       0);
   } else {
     CwtBatchOp<float2, float2> op{};
-    run_cwt_batch_f32(op, nsig, max_na, m, nullptr, zbytes / sizeof(float2), tb, 0);
+    op.band_from = band_from;
+    run_cwt_batch_f32(op, nsig, max_na, m, band_log, nullptr, zbytes / sizeof(float2), tb, 0);
   }
   set_launch_counter(nullptr);
   return count;
+}
+
+int ssqb_cwt_batch_launches(const ssqb_sig* sigs, int nsig, int Npad, int precision,
+                            size_t workspace_bytes) {
+  return cwt_batch_launches_impl(sigs, nsig, Npad, precision, workspace_bytes, 0x7fffffff, 0);
+}
+
+int ssqb_cwt_batch_ex_launches(const ssqb_sig* sigs, int nsig, int Npad, int precision,
+                               size_t workspace_bytes, int band_from, int band_log) {
+  if (band_from < 0 || band_log < 0 || band_log > band_log_max(precision)) return -1;
+  return cwt_batch_launches_impl(sigs, nsig, Npad, precision, workspace_bytes, band_from,
+                                 band_log);
 }
 
 int ssqb_squeeze_batch(const void* Wx, const uint16_t* idx, const ssqb_sig* sigs,

@@ -1,11 +1,11 @@
 // Mixed-radix shared-memory Stockham FFT for transform lengths M that are a
-// power of two times 3 or 5 (the chirp-z transform of an n_fft that is not a
-// power of two needs M >= 2 n_fft - 1; M = 1280 = 5 * 8 * 8 * 4 instead of
-// 2048 for n_fft 598). The same autosort stage as fft_tile.cuh with any radix
+// power of two times 5 (the chirp-z transform of an n_fft that is not a
+// power of two needs M >= 2 n_fft - 1: M = 1280 = 5 * 4^4 instead of 2048 for
+// n_fft 598). The same autosort stage as fft_tile.cuh with any radix
 // R of a compile-time radix list:
 //   v[r] = x[j + r*M/R] * w_{NS*R}^{r*(j mod NS)},  v = DFT_R(v),
 //   y[(j div NS)*NS*R + (j mod NS) + r*NS] = v[r],  NS = product of the
-// previous radices, w_{NS*R}^e = W[e * M/(NS*R) mod M] from a table
+// previous radices, w_{NS*R}^e = W[e * M/(NS*R)] from a table
 // W[m] = exp(2 pi i m / M) in shared memory. One array, NF rows of M per
 // CTA; inputs through the caller's loader, outputs left in shared memory.
 #pragma once
@@ -24,21 +24,9 @@ struct Radices {
   }
 };
 
-// DFT of 3 or 5 points, sign SIGN, natural order (from the definition
-// y_k = sum_n x_n e^{SIGN 2 pi i n k / R}, sums and differences of the
+// DFT of 5 points, sign SIGN, natural order (from the definition
+// y_k = sum_n x_n e^{SIGN 2 pi i n k / 5}, sums and differences of the
 // symmetric pairs first)
-template <int SIGN, typename C>
-__device__ __forceinline__ void dft3(C (&v)[3]) {
-  typedef typename RealOf<C>::type T;
-  const T c = (T)-0.5;                                   // cos(2 pi / 3)
-  const T s = (T)(SIGN * 0.86602540378443864676);       // SIGN sin(2 pi / 3)
-  const C a = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-  const C m = mk(v[0].x + c * a.x, v[0].y + c * a.y);
-  v[0] = cadd(v[0], a);
-  v[1] = mk(m.x - s * d.y, m.y + s * d.x);
-  v[2] = mk(m.x + s * d.y, m.y - s * d.x);
-}
-
 template <int SIGN, typename C>
 __device__ __forceinline__ void dft5(C (&v)[5]) {
   typedef typename RealOf<C>::type T;
@@ -62,8 +50,7 @@ __device__ __forceinline__ void dft5(C (&v)[5]) {
 
 template <int R, int SIGN, typename C>
 __device__ __forceinline__ void dft_any(C (&v)[R]) {
-  if constexpr (R == 3) dft3<SIGN>(v);
-  else if constexpr (R == 5) dft5<SIGN>(v);
+  if constexpr (R == 5) dft5<SIGN>(v);
   else dft<R, SIGN>(v);
 }
 

@@ -120,16 +120,30 @@ int run_xhat_batch_f32(const float* x, const SigDesc* desc, int nsig, int Npad, 
                                                     st);
 }
 
+// rows [0, band_from) by the tile passes, [band_from, max_na) by the band pass
+template <class BOp, typename C>
+static int run_cwt_batch_t(const BOp& op, int nsig, int max_na, int log2L, int band_log,
+                           C* Z, size_t zcap, const Tables& tb, cudaStream_t st) {
+  const int bf = op.band_from < max_na && two_pass<C>(log2L) ? op.band_from : max_na;
+  if (bf > 0) {
+    const int e = run_batch<BOp, C, 1>(op, nsig, bf, log2L, Z, zcap, tb, st);
+    if (e) return e;
+  }
+  if (bf < max_na)
+    return run_band<BOp, C, 1>(op, nsig, log2L, band_log, Z, zcap, bf, max_na - bf, tb, st);
+  return 0;
+}
+
 int run_cwt_batch_f32x(const CwtBatchOp<double2, float2>& op, int nsig, int max_na,
-                       int log2L, double2* Z, size_t zcap, const Tables& tb, cudaStream_t st) {
-  return run_batch<CwtBatchOp<double2, float2>, double2, 1>(op, nsig, max_na, log2L, Z, zcap,
-                                                            tb, st);
+                       int log2L, int band_log, double2* Z, size_t zcap, const Tables& tb,
+                       cudaStream_t st) {
+  return run_cwt_batch_t(op, nsig, max_na, log2L, band_log, Z, zcap, tb, st);
 }
 
 int run_cwt_batch_f32(const CwtBatchOp<float2, float2>& op, int nsig, int max_na, int log2L,
-                      float2* Z, size_t zcap, const Tables& tb, cudaStream_t st) {
-  return run_batch<CwtBatchOp<float2, float2>, float2, 1>(op, nsig, max_na, log2L, Z, zcap,
-                                                          tb, st);
+                      int band_log, float2* Z, size_t zcap, const Tables& tb,
+                      cudaStream_t st) {
+  return run_cwt_batch_t(op, nsig, max_na, log2L, band_log, Z, zcap, tb, st);
 }
 
 }  // namespace ssqb

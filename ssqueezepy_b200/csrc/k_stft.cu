@@ -160,16 +160,12 @@ static int launch_bluestein(const StftOp<TX, double2, OC>& op, int B, const Tabl
 // (mixed-radix Stockham, fft_mixed.cuh) where that is shorter than the power
 // of two: n_fft 598 convolves at 1280 instead of 2048. The twiddle table
 // W[m] = exp(2 pi i m / M) is filled once per (persistent) CTA.
-// threads of the mixed-radix kernel, and the radix schedule of 1280
-#ifndef SSQB_BLU_NT
-#define SSQB_BLU_NT 256
-#endif
-#ifndef SSQB_BLU_R1280
-#define SSQB_BLU_R1280 0
-#endif
-constexpr int kBluNT = SSQB_BLU_NT;
-typedef std::conditional_t<SSQB_BLU_R1280 == 0, Radices<5, 8, 8, 4>, Radices<5, 4, 4, 4, 4>>
-    Radices1280;
+// 320 threads: the radix-4 stages of 1280 = 5 x 4^4 have 320 items each
+// (measured at n_fft 598: 7.30 ms per N=160,000 ssq_stft against 7.72 at the
+// power of two 2048; 256 threads with 5 x 8 x 8 x 4: 9.40, 160 threads:
+// 8.24; 1536 = 3 x 8^3 for n_fft 700: 11.5 against 8.2 at 2048, not used)
+constexpr int kBluNT = 320;
+typedef Radices<5, 4, 4, 4, 4> Radices1280;
 
 template <typename TX, typename OC, int M, class RL>
 __global__ void __launch_bounds__(kBluNT, kBluesteinCtas)
@@ -276,33 +272,20 @@ static int launch_bluestein_mixed(const StftOp<TX, double2, OC>& op, int B, cons
   return cudaGetLastError();
 }
 
-// Convolution length of the chirp-z transform of an n_fft of L: the smallest
-// of 2^k, 3 * 2^k (>= 192) and 5 * 2^k (>= 160) that is >= 2L - 1 and fits
-// the float64 tile.
-#ifndef SSQB_BLU_MIXED
-#define SSQB_BLU_MIXED 1
-#endif
+// Convolution length of the chirp-z transform of an n_fft of L: 1280 where
+// that suffices and the power of two would be 2048 (n_fft 513-640), else the
+// smallest power of two >= 2L - 1.
 static int bluestein_length(int L) {
-  int best = 1 << 30;
-  for (int f : {1, 3, 5})
-    if (f == 1 || SSQB_BLU_MIXED)
-    for (int m = f * 8; m <= tile_of<double2>(); m *= 2)
-      if (m >= 2 * L - 1 && m < best && (f == 1 || m >= 160)) best = m;
-  return best;
+  int m = 8;
+  while (m < 2 * L - 1) m *= 2;
+  return (m == 2048 && 2 * L - 1 <= 1280) ? 1280 : m;
 }
 
 template <typename TX, typename OC>
 static int run_bluestein(const StftOp<TX, double2, OC>& op, int B, int log2M,
                          const Tables& tb, cudaStream_t st) {
   switch (bluestein_length(op.L)) {
-    case 160: return launch_bluestein_mixed<TX, OC, 160, Radices<5, 8, 4>>(op, B, tb, st);
-    case 192: return launch_bluestein_mixed<TX, OC, 192, Radices<3, 8, 8>>(op, B, tb, st);
-    case 320: return launch_bluestein_mixed<TX, OC, 320, Radices<5, 8, 8>>(op, B, tb, st);
-    case 384: return launch_bluestein_mixed<TX, OC, 384, Radices<3, 8, 4, 4>>(op, B, tb, st);
-    case 640: return launch_bluestein_mixed<TX, OC, 640, Radices<5, 8, 4, 4>>(op, B, tb, st);
-    case 768: return launch_bluestein_mixed<TX, OC, 768, Radices<3, 8, 8, 4>>(op, B, tb, st);
     case 1280: return launch_bluestein_mixed<TX, OC, 1280, Radices1280>(op, B, tb, st);
-    case 1536: return launch_bluestein_mixed<TX, OC, 1536, Radices<3, 8, 8, 8>>(op, B, tb, st);
     default:
       return dispatch_log<3, tile_log<double2>()>(log2M, [&](auto k) {
         return launch_bluestein<TX, OC, decltype(k)::value>(op, B, tb, st);

@@ -129,10 +129,13 @@ int run_trigdiff(const void* A, bool f64, int rows, int M, int Npad, int n1, int
 int run_xhat_batch_f32(const float* x, const SigDesc* desc, int nsig, int Npad, int padtype,
                        double2* xh, double2* Z, size_t zcap, const Tables& tb,
                        cudaStream_t st);
+// op.band_from < max_na: rows from there take the band pass at 2^band_log bins
 int run_cwt_batch_f32x(const CwtBatchOp<double2, float2>& op, int nsig, int max_na,
-                       int log2L, double2* Z, size_t zcap, const Tables& tb, cudaStream_t st);
+                       int log2L, int band_log, double2* Z, size_t zcap, const Tables& tb,
+                       cudaStream_t st);
 int run_cwt_batch_f32(const CwtBatchOp<float2, float2>& op, int nsig, int max_na, int log2L,
-                      float2* Z, size_t zcap, const Tables& tb, cudaStream_t st);
+                      int band_log, float2* Z, size_t zcap, const Tables& tb,
+                      cudaStream_t st);
 int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* desc,
                           int nsig, int max_na, int max_N, float2* Tx, int* status,
                           cudaStream_t st);

@@ -546,12 +546,22 @@ struct CwtBatchOp {
   OC* Wx;
   uint16_t* idx;
   int* status;
+  int band_from = 0x7fffffff;  // rows from here take the band-limited pass
   __device__ CwtOp<C, OC> bind(int b) const {
     const SigDesc& d = desc[b];
     const BinDev bd{d.mode, d.idx1, d.flipud, d.nbins, d.p0, d.p1, d.p2, d.p3};
-    return CwtOp<C, OC>{xh + (size_t)b * Npad, d.scales, wav, bd, d.na, d.N, Npad, d.n1,
-                        h, inv_dt, inv_npad, gamma, Wx + d.out_off, nullptr, nullptr,
-                        idx + d.idx_off, d.idx_pitch, status};
+    CwtOp<C, OC> o{xh + (size_t)b * Npad, d.scales, wav, bd, d.na, d.N, Npad, d.n1,
+                   h, inv_dt, inv_npad, gamma, Wx + d.out_off, nullptr, nullptr,
+                   idx + d.idx_off, d.idx_pitch, status};
+    o.nrun = d.na < band_from ? d.na : band_from;
+    return o;
+  }
+  // the same op for signals b0, b0+1, ... (descriptors and spectra advanced)
+  __host__ __device__ CwtBatchOp shifted(int b0) const {
+    CwtBatchOp o = *this;
+    o.desc += b0;
+    o.xh += (size_t)b0 * Npad;
+    return o;
   }
 };
 

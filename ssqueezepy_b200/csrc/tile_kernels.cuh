@@ -342,6 +342,7 @@ band_prep(Op op, C* __restrict__ Zb, int row0, int nrows, int logM) {
   const auto bop = op.bind(blockIdx.z);
   const int b = Op::kBatch ? 0 : blockIdx.z;
   const int row = row0 + blockIdx.x;
+  if (row >= bop.na) return;  // signals with fewer rows (uneven batches)
   const int M = 1 << logM;
   int klo, khi;
   bop.band_bins(row, klo, khi);
@@ -444,6 +445,7 @@ band_single(Op op, Tables tb, const C* __restrict__ Zb, int log2L, int row0, int
   const auto bop = op.bind(blockIdx.z);
   const int b = Op::kBatch ? 0 : blockIdx.z;
   const int row = row0 + blockIdx.y;
+  if (row >= bop.na) return;
   int klo, khi;
   bop.band_bins(row, klo, khi);
   const C* zb = Zb + ((size_t)blockIdx.z * nrows + blockIdx.y) * NARR * M;

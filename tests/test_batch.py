@@ -251,3 +251,29 @@ def test_full_uneven_batch_every_signal_against_oracle():
     assert errs[:, 0].max() <= 1e-5
     assert errs[:, 1].max() <= 1e-4
     assert L.device_status() == 0
+
+
+@pytest.mark.gpu
+def test_batch_band_pass_equals_tile_passes():
+    """Rows whose wavelet band fits 512 bins take the band-limited single pass
+    (ssqb_cwt_batch_ex); with it switched off every row takes the tile
+    passes. Both compute in float64, so Wx agrees to float32 rounding and the
+    bins agree except at exact ties."""
+    torch = _gpu()
+    from ssqueezepy_b200._batch import SsqCwtBatch
+    rng = np.random.default_rng(21)
+    lengths = [5000, 9000, 20000, 33000, 60000]
+    xs = [S.chirp_mix(N, rng).astype(np.float32) for N in lengths]
+    plan = SsqCwtBatch(lengths, wavelet=('morlet', {'mu': 6.}))
+    assert any(g['band'][0] < (1 << 30) for g in plan.groups)
+    band = [(t.clone(), w.clone()) for t, w, _, _ in plan(xs)]
+    idx_band = plan.idx.clone()
+    for g in plan.groups:
+        g['band'] = (1 << 30, 0)
+    tile = [(t.clone(), w.clone()) for t, w, _, _ in plan(xs)]
+    torch.cuda.synchronize()
+    for (t1, w1), (t0, w0) in zip(band, tile):
+        assert (w1 - w0).norm() <= 1e-7 * w0.norm()
+        assert (t1 - t0).norm() <= 1e-6 * t0.norm()
+    assert int((idx_band != plan.idx).sum()) <= 2
+    assert L.device_status() == 0

@@ -72,11 +72,11 @@ def test_default_n_fft_of_a_short_signal():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('n_fft, M', [(80, 160), (90, 192), (300, 640), (700, 1536)])
-def test_stft_mixed_radix_lengths_match_oracle(n_fft, M):
-    """n_fft whose chirp-z convolution takes a mixed-radix length M (3 or 5
-    times a power of two, shorter than the power of two): Sx, dSx against the
-    float64 oracle, hop 1 and 3."""
+@pytest.mark.parametrize('n_fft', [513, 600, 640])
+def test_stft_mixed_radix_lengths_match_oracle(n_fft):
+    """n_fft 513-640: the chirp-z convolution runs at the mixed-radix length
+    1280 = 5 x 4^4 instead of 2048. Sx, dSx against the float64 oracle, hop
+    1 and 3 (the reference's benchmark length 598 is in the golden cases)."""
     sb = _gpu()
     from oracle import ssq_oracle as O
     from ssqueezepy_b200 import _params as P
@@ -86,5 +86,5 @@ def test_stft_mixed_radix_lengths_match_oracle(n_fft, M):
         Sx, dSx = sb.stft(x, 'hann', n_fft=n_fft, hop_len=hop, derivative=True,
                           dtype='float64')
         So, dSo = O.stft(x, win, dwin, n_fft, hop=hop)
-        assert rel_l2(Sx.cpu().numpy(), So) <= 1e-11, (n_fft, M, hop)
-        assert rel_l2(dSx.cpu().numpy(), dSo) <= 1e-11, (n_fft, M, hop)
+        assert rel_l2(Sx.cpu().numpy(), So) <= 1e-11, (n_fft, hop)
+        assert rel_l2(dSx.cpu().numpy(), dSo) <= 1e-11, (n_fft, hop)
