@@ -124,13 +124,15 @@ int run_xhat_batch_f32(const float* x, const SigDesc* desc, int nsig, int Npad, 
 template <class BOp, typename C>
 static int run_cwt_batch_t(const BOp& op, int nsig, int max_na, int log2L, int band_log,
                            C* Z, size_t zcap, const Tables& tb, cudaStream_t st) {
-  const int bf = op.band_from < max_na && two_pass<C>(log2L) ? op.band_from : max_na;
+  BOp o = op;  // single-pass lengths and no band rows: every row by the tile passes
+  if (!(op.band_from < max_na && two_pass<C>(log2L))) o.band_from = 0x7fffffff;
+  const int bf = o.band_from < max_na ? o.band_from : max_na;
   if (bf > 0) {
-    const int e = run_batch<BOp, C, 1>(op, nsig, bf, log2L, Z, zcap, tb, st);
+    const int e = run_batch<BOp, C, 1>(o, nsig, bf, log2L, Z, zcap, tb, st);
     if (e) return e;
   }
   if (bf < max_na)
-    return run_band<BOp, C, 1>(op, nsig, log2L, band_log, Z, zcap, bf, max_na - bf, tb, st);
+    return run_band<BOp, C, 1>(o, nsig, log2L, band_log, Z, zcap, bf, max_na - bf, tb, st);
   return 0;
 }
 
