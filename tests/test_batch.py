@@ -212,11 +212,22 @@ def test_batch_autotune_picks_a_budget_and_keeps_results():
            SsqCwtBatch(LENGTHS, wavelet=('morlet', {'mu': 6.}))(xs)]
     plan = SsqCwtBatch(LENGTHS, wavelet=('morlet', {'mu': 6.}), autotune=True, graph=True)
     assert plan.tuning and all(t['ms'] for t in plan.tuning)
+    first = None
     for _ in range(2):
         outs = plan(xs)
         torch.cuda.synchronize()
+        # the tuned band bound may send other rows through the band pass: the
+        # same float64 transform summed in another order, so equal to float32
+        # rounding, and replays of the tuned plan equal each other exactly
         for (t, w, _, _), (t0, w0) in zip(outs, ref):
-            assert torch.equal(t, t0) and torch.equal(w, w0)
+            assert (w - w0).norm() <= 1e-7 * w0.norm()
+            assert (t - t0).norm() <= 1e-6 * t0.norm()
+        cur = [(t.clone(), w.clone()) for t, w, _, _ in outs]
+        if first is not None:
+            assert all(torch.equal(a, b) and torch.equal(c, d)
+                       for (a, c), (b, d) in zip(cur, first))
+        first = cur
+    assert all('band_bins' in t for t in plan.tuning)
     assert L.device_status() == 0
 
 
