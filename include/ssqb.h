@@ -126,9 +126,10 @@ SSQB_API int ssqb_cwt(const void* x, int B, int N, int Npad, int n1, int padtype
 
 /* ssqb_cwt with the scale values also given on the host (`scales_host`, na
  * doubles equal to the device `scales`; NULL makes it ssqb_cwt). They let
- * the call plan per row: rows whose wavelet band spans at most a quarter of
- * a transform tile (512 bins with float64 arithmetic, 1024 with SSQB_F32) go
- * through a band-limited single pass (D = Npad / M transforms of the
+ * the call plan per row: rows whose wavelet band spans at most half a
+ * transform tile for Npad <= 65536, a quarter above (1024 / 512 bins with
+ * float64 arithmetic, 2048 / 1024 with SSQB_F32), go through a band-limited
+ * single pass (D = Npad / M transforms of the
  * twiddled band, M the band's power-of-two length, no two-pass
  * intermediate) instead of the four-step of the full padded length. Same
  * outputs, workspace and stream semantics as ssqb_cwt. No reference
@@ -313,8 +314,8 @@ SSQB_API int ssqb_cwt_batch_ex_launches(const ssqb_sig* sigs, int nsig, int Npad
  * band-limited single pass: the first such row (`band_from`, na if none; the
  * rest of the rows are such too) and the power of two of their largest band
  * (`band_log`, 0 if none). max_bins: the largest band length allowed (a power
- * of two of at most half a tile; 0 = the ssqb_cwt_ex default, 512 bins with
- * float64 arithmetic). No reference counterpart. */
+ * of two of at most half a tile; 0 = the ssqb_cwt_ex default for this
+ * Npad). No reference counterpart. */
 SSQB_API int ssqb_cwt_band_rows(const double* scales_host, int na, int Npad,
                                 const ssqb_wavelet* wavelet, int precision, int max_bins,
                                 int* band_from, int* band_log);

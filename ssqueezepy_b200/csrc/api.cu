@@ -203,12 +203,11 @@ static int check_sigs(const ssqb_sig* s, int nsig, int Npad, bool need_scales,
   return SSQB_OK;
 }
 
-// band rows: bands of at most TILE / 2^SSQB_BAND_OFF bins, i.e.
-// 2^SSQB_BAND_OFF residues per CTA of the single pass (512 bins with float64
-// arithmetic measured faster than 256 or 1024 at N = 10,000 and 160,000)
-#ifndef SSQB_BAND_OFF
-#define SSQB_BAND_OFF 2
-#endif
+// band rows: bands of at most TILE / 2^off bins (2^off residues per CTA of
+// the single pass). With float64 arithmetic 1024 bins (off 1) measured
+// fastest up to Npad = 65,536 and 512 (off 2) above (single calls at N =
+// 10,000 / 60,000 / 160,000, and the batch autotuner's choices per length)
+static int band_off(int Npad) { return Npad <= (1 << 16) ? 1 : 2; }
 // Rows whose wavelet band fits at most 2^max_log bins, as band_bins
 // evaluates it on the device (the same float64 expressions): the longest
 // suffix of such rows takes the band-limited single pass. No host scales:
@@ -331,7 +330,7 @@ int ssqb_cwt_ex_launches(int B, int Npad, int na, int precision, size_t workspac
   if (!scales_host || check_wavelet(wavelet, &wd)) return -1;
   BandPlan bp{};
   const int max_log = ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE
-                                                  : FftCfg<double2>::TILE) - SSQB_BAND_OFF;
+                                                  : FftCfg<double2>::TILE) - band_off(Npad);
   cwt_band_plan(scales_host, na, Npad, wd, max_log, &bp);
   return cwt_launches_impl(B, Npad, na, precision, workspace_bytes, &bp);
 }
@@ -387,7 +386,7 @@ static int cwt_impl(const void* x, int B, int N, int Npad, int n1, int padtype, 
   const int oN = rpadded ? Npad : N, on1 = rpadded ? 0 : n1;
   BandPlan bp{};
   const int max_log = ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE
-                                                  : FftCfg<double2>::TILE) - SSQB_BAND_OFF;
+                                                  : FftCfg<double2>::TILE) - band_off(Npad);
   cwt_band_plan(scales_host, na, Npad, wd, max_log, &bp);
   if (precision == SSQB_F32) {
     CwtOp<float2> op{xh, scales, wd, bd, na, oN, Npad, on1, h, 1.0 / dt,
@@ -763,7 +762,7 @@ int ssqb_cwt_band_rows(const double* scales_host, int na, int Npad,
   int r = check_wavelet(wavelet, &wd);
   if (r) return r;
   int max_log = ilog2i(precision == SSQB_F32 ? FftCfg<float2>::TILE
-                                             : FftCfg<double2>::TILE) - SSQB_BAND_OFF;
+                                             : FftCfg<double2>::TILE) - band_off(Npad);
   if (max_bins > 0) {
     if (!is_pow2(max_bins) || ilog2i(max_bins) > band_log_max(precision))
       return fail(SSQB_EINVAL, "max_bins must be a power of two of at most half a tile");
