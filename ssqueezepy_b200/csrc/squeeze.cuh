@@ -10,14 +10,17 @@
 
 namespace ssqb {
 
+// Sources give the bin of entry (row, j) of Wx, at flat offset o = row * N + j
+// (row counts over all signals' rows): pre() issues its loads, bin() decodes.
+
 // bin from a precomputed uint16 index (kNoBin = masked)
 template <typename C>
 struct IdxSrc {
   const uint16_t* idx;
   int pitch, N;  // idx rows of `pitch` columns; Wx rows of N
   struct Pre { uint16_t k; };
-  __device__ __forceinline__ Pre pre(size_t o) const {
-    return Pre{__ldg(idx + (o / N) * pitch + o % N)};
+  __device__ __forceinline__ Pre pre(size_t, size_t row, int j) const {
+    return Pre{__ldg(idx + row * pitch + j)};
   }
   __device__ __forceinline__ int bin(const Pre& p, C, int) const {
     return p.k == kNoBin ? -1 : (int)p.k;
@@ -33,7 +36,7 @@ struct PhaseSrc {
   double gamma;
   int* status;
   struct Pre { C d; };
-  __device__ __forceinline__ Pre pre(size_t o) const { return Pre{dWx[o]}; }
+  __device__ __forceinline__ Pre pre(size_t o, size_t, int) const { return Pre{dWx[o]}; }
   __device__ __forceinline__ int bin(const Pre& p, C v, int i) const {
     const uint16_t k = phase_bin(v, p.d, sfs ? sfs[i] : 0.0, sfs != nullptr, bins,
                                  gamma, status, nullptr);
@@ -50,7 +53,7 @@ struct WSrc {
   BinDev bins;
   int* status;
   struct Pre { T w; };
-  __device__ __forceinline__ Pre pre(size_t o) const { return Pre{w[o]}; }
+  __device__ __forceinline__ Pre pre(size_t o, size_t, int) const { return Pre{w[o]}; }
   __device__ __forceinline__ int bin(const Pre& p, C, int) const {
     if (isinf(p.w)) return -1;
     const int k = bin_of(bins, (double)p.w);
@@ -81,7 +84,8 @@ __device__ __forceinline__ void squeeze_body(const C* __restrict__ Wx, const Src
   for (int k = lane; k < nbins * CW; k += 32) acc[k] = mk((T)0, (T)0);
   for (int i = lane; i < na; i += 32) cs[i] = (T)cst[i];
   __syncwarp();
-  const size_t base = (size_t)b * na * N + j;
+  const size_t row0 = (size_t)b * na;
+  const size_t base = row0 * N + j;
   for (int i0 = 0; i0 < na; i0 += G * U) {
     C v[U];
     typename Src::Pre p[U];
@@ -93,7 +97,7 @@ __device__ __forceinline__ void squeeze_body(const C* __restrict__ Wx, const Src
       if (ok[u]) {
         const size_t o = base + (size_t)i * N;
         v[u] = Wx[o];
-        p[u] = src.pre(o);
+        p[u] = src.pre(o, row0 + i, j);
       }
     }
 #pragma unroll
