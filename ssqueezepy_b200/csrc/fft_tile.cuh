@@ -155,12 +155,6 @@ template <> __device__ __forceinline__ const double2* seg_table<double2>(const T
 // A loader with `kGather` gathers the R inputs of one first-stage item at
 // once (`gather<R>(f, j, stride, t)`: inputs j + r*stride of row f), so that
 // it can issue all of its memory loads before the arithmetic on them.
-// A loader with `kSmem` reads the stage buffers themselves: the first stage
-// then waits for every thread's reads before it overwrites them.
-template <class T, class = void> struct LoadsSmem : std::false_type {};
-template <class T>
-struct LoadsSmem<T, std::void_t<decltype(T::kSmem)>> : std::bool_constant<T::kSmem> {};
-
 template <class T, class = void> struct HasGather : std::false_type {};
 template <class T>
 struct HasGather<T, std::void_t<decltype(T::kGather)>> : std::bool_constant<T::kGather> {};
@@ -221,7 +215,7 @@ __device__ __forceinline__ void fft_stage(C* const (&buf)[NARR], const C* __rest
       }
     }
   }
-  if constexpr ((!FIRST || LoadsSmem<LD>::value) && !(LAST && DIRECT_OUT)) __syncthreads();
+  if constexpr (!FIRST && !(LAST && DIRECT_OUT)) __syncthreads();
   // twiddle, butterfly, scatter
 #pragma unroll
   for (int p = 0; p < PER; ++p) {

@@ -6,14 +6,19 @@ namespace ssqb {
 
 // Lane layout G (rows per warp instruction): the accumulator of a warp is
 // nbins x 32/G; G = 4 keeps it small enough for about ten warps per SM.
-// U: row groups whose loads are issued together. Measured at N = 160,000 /
-// 60,000 (293 / 277 rows): U = 8 0.373 / 0.139 ms, 4: 0.562 / 0.213,
-// 12: 0.48 / 0.18, 16: 0.436 / 0.172.
+// U: row groups whose loads are issued together. Measured, one signal at
+// N = 160,000 / 60,000 (293 / 277 rows): U = 8 0.373 / 0.139 ms, 4: 0.562 /
+// 0.213, 12: 0.48 / 0.18, 16: 0.436 / 0.172. The batch kernel (per-signal
+// descriptors) over 256 signals of 4,096-65,536 samples: U = 16 25.5 ms,
+// 8: 38.6, 12: 40.1.
 #ifndef SSQB_SQ_G
 #define SSQB_SQ_G 4
 #endif
 #ifndef SSQB_SQ_U
 #define SSQB_SQ_U 8
+#endif
+#ifndef SSQB_SQB_U
+#define SSQB_SQB_U 16
 #endif
 
 template <typename C, class Src>
@@ -58,7 +63,7 @@ int run_squeeze_batch_f32(const float2* Wx, const uint16_t* idx, const SigDesc* 
                           int nsig, int max_na, int max_N, float2* Tx, int* status,
                           cudaStream_t st) {
   if (int* c = launch_counter()) return ++*c, 0;
-  constexpr int G = SSQB_SQ_G, U = SSQB_SQ_U, CW = 32 / G;
+  constexpr int G = SSQB_SQ_G, U = SSQB_SQB_U, CW = 32 / G;
   const size_t smem = (size_t)max_na * CW * sizeof(float2) + (size_t)max_na * sizeof(float);
   auto k = squeeze_batch_kernel<float2, G, U>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,

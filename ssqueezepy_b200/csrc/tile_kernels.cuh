@@ -32,11 +32,6 @@ template <typename C> __host__ __device__ constexpr int tile_of() {
 #ifndef SSQB_FP64_MINBLOCKS
 #define SSQB_FP64_MINBLOCKS 2
 #endif
-// Pass 1 of split-load ops forms its inputs in shared memory first (1) or
-// gathers them per butterfly item (0).
-#ifndef SSQB_P1_STAGE
-#define SSQB_P1_STAGE 0
-#endif
 template <typename C> struct MinBlocks { static constexpr int v = 2; };
 template <> struct MinBlocks<double2> { static constexpr int v = SSQB_FP64_MINBLOCKS; };
 
@@ -114,18 +109,6 @@ struct P1Loader<BOp, C, NARR, std::enable_if_t<BOp::kSplitLoad>> {
   __device__ __forceinline__ void operator()(int f, int m, C (&v)[NARR]) const {
     op.load(b, row, k1_0 + f + L1 * m, v);
   }
-  // input m of column k1_0 + f alone (spectrum load, wavelet, products)
-  __device__ __forceinline__ void one(int f, int m, C (&v)[NARR]) const {
-    const int k = k1_0 + f + L1 * m;
-    const int kk = (k <= (op.Npad >> 1)) ? k : k - op.Npad;
-    if (kk >= klo && kk <= khi) {
-      op.apply(k, op.raw(b, k, klo, khi), op.psi(row, k), v);
-    } else {
-#pragma unroll
-      for (int a = 0; a < NARR; ++a)
-        v[a] = mk((typename RealOf<C>::type)0, (typename RealOf<C>::type)0);
-    }
-  }
   template <int R>
   __device__ __forceinline__ void gather(int f, int j, int stride, C (&t)[R][NARR]) const {
     double2 raw[R];
@@ -153,17 +136,6 @@ struct P1Loader<BOp, C, NARR, std::enable_if_t<BOp::kSplitLoad>> {
       for (int r = 0; r < R; ++r)
         op.finish(b, row, k1_0 + f + L1 * (j + r * stride), raw[r], t[r]);
     }
-  }
-};
-
-// Loader of the stage buffers themselves (inputs staged in natural order).
-template <typename C, int NARR, class LY>
-struct SmemLoader {
-  static constexpr bool kSmem = true;
-  C* const (&buf)[NARR];
-  __device__ __forceinline__ void operator()(int f, int m, C (&v)[NARR]) const {
-#pragma unroll
-    for (int a = 0; a < NARR; ++a) v[a] = buf[a][LY::at(f, m)];
   }
 };
 
@@ -270,25 +242,7 @@ tile_pass1(Op op, Tables tb, C* __restrict__ Z, int log2L, int row_lo, int rows_
     }
   }
   Pass1Store<C, NARR, SIGN> st{tb, zrow, k1_0, L1, log2L};
-  if constexpr (HasGather<P1Loader<BOp, C, NARR>>::value && SSQB_P1_STAGE) {
-    // The CTA's inputs (spectrum x wavelet, both arrays) are formed first in
-    // one rolled loop, in shared memory, and the transform reads them from
-    // there: one copy of the wavelet code, and the spectrum loads of a
-    // thread's elements overlap the wavelet arithmetic of the others.
-#pragma unroll 2
-    for (int e = threadIdx.x; e < NF * L2; e += kNT) {
-      const int f = e % NF, m = e / NF;
-      C v[NARR];
-      ld.one(f, m, v);
-#pragma unroll
-      for (int a = 0; a < NARR; ++a) buf[a][LY::at(f, m)] = v[a];
-    }
-    __syncthreads();
-    SmemLoader<C, NARR, LY> sl{buf};
-    fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), sl, st);
-  } else {
-    fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
-  }
+  fft_rows<C, LOGL2, NF, kNT, SIGN, NARR, MAP_F, MAP_F, true>(buf, seg_table<C>(tb), ld, st);
 }
 
 // pass 2: CTA = (n2 block of NF = TILE/L1 values, row, batch item).
