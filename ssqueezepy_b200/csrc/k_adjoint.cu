@@ -26,6 +26,9 @@ struct AdjRowOp {
   static constexpr int NARR = 1;
   static constexpr bool kDirect = true;
   static constexpr bool kBatch = false;
+  // one copy of the wavelet evaluation in the store: 37.10 vs 37.43 ms for
+  // the 64 x 16,384 forward + backward, same gradients
+  static constexpr bool kRolledStore = true;
   AdjSources<C> src;
   const double* scales;
   WavDev wav;

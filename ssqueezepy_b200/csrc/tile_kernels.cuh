@@ -35,6 +35,13 @@ template <typename C> __host__ __device__ constexpr int tile_of() {
 template <typename C> struct MinBlocks { static constexpr int v = 2; };
 template <> struct MinBlocks<double2> { static constexpr int v = SSQB_FP64_MINBLOCKS; };
 
+// An op with `kRolledStore` has its outputs stored in a rolled loop: one
+// copy of a long store (e.g. a wavelet evaluation) instead of R.
+template <class T, class = void> struct RolledStore : std::false_type {};
+template <class T>
+struct RolledStore<T, std::void_t<decltype(T::kRolledStore)>>
+    : std::bool_constant<T::kRolledStore> {};
+
 // Storer handing each output to op.store. Single pass: row = row0 + f,
 // index m; pass 2: row fixed, index L2*m + n2_0 + f (mul = L2, add = n2_0).
 template <class Op, typename C>
@@ -47,13 +54,19 @@ struct StoreEach {
     const bool single = (nrows != 0x7fffffff);
     const int row = single ? row0 + f : row0;
     if (single && row >= nrows) return;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
+    auto one = [&](int r) {
       C v[NARR];
       v[0] = a[r];
       v[NARR - 1] = z[r];
       const int m = m0 + r * stride;
       op.store(b, row, single ? m : mul * m + add + f, v);
+    };
+    if constexpr (RolledStore<Op>::value) {
+#pragma unroll 1
+      for (int r = 0; r < R; ++r) one(r);
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) one(r);
     }
   }
 };
