@@ -159,7 +159,7 @@ static int launch_bluestein(const StftOp<TX, double2, OC>& op, int B, const Tabl
 // The same chirp-z transform with a convolution length M = 3 * 2^k or 5 * 2^k
 // (mixed-radix Stockham, fft_mixed.cuh) where that is shorter than the power
 // of two: n_fft 598 convolves at 1280 instead of 2048. The twiddle table
-// W[m] = exp(2 pi i m / M) is filled once per (persistent) CTA.
+// W[m] = exp(2 pi i m / M) (at tw_pos(m)) is filled once per (persistent) CTA.
 // 320 threads: the radix-4 stages of 1280 = 5 x 4^4 have 320 items each
 // (measured at n_fft 598: 7.30 ms per N=160,000 ssq_stft against 7.72 at the
 // power of two 2048; 256 threads with 5 x 8 x 8 x 4: 9.40, 160 threads:
@@ -185,7 +185,7 @@ stft_bluestein_mixed_kernel(StftOp<TX, double2, OC> op, Tables tb) {
   for (int m = threadIdx.x; m < M; m += kBluNT) {
     double sv, cv;
     sincospi((double)(2 * m) / (double)M, &sv, &cv);
-    W[m] = make_double2(cv, sv);
+    W[tw_pos(m)] = make_double2(cv, sv);
   }
   __syncthreads();
   auto ldB = [&](int, int m, C (&v)[1]) {
