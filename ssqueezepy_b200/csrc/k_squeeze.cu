@@ -9,8 +9,10 @@ namespace ssqb {
 // U: row groups whose loads are issued together. Measured, one signal at
 // N = 160,000 / 60,000 (293 / 277 rows): U = 8 0.373 / 0.139 ms, 4: 0.562 /
 // 0.213, 12: 0.48 / 0.18, 16: 0.436 / 0.172. The batch kernel (per-signal
-// descriptors) over 256 signals of 4,096-65,536 samples: U = 16 25.5 ms,
-// 8: 38.6, 12: 40.1.
+// descriptors) over 256 signals of 4,096-65,536 samples, whose Wx comes
+// mostly from DRAM: U = 16 25.5 ms, 8: 38.6, 12: 40.1; with the next 16 row
+// groups' loads in flight during the updates (PIPE) 22.2 ms. The one-signal
+// kernel with PIPE: 0.379 ms (U = 8) / 0.371 (U = 4) against 0.373.
 #ifndef SSQB_SQ_G
 #define SSQB_SQ_G 4
 #endif

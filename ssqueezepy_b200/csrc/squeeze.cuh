@@ -66,8 +66,9 @@ struct WSrc {
 // handles column j0 + c of rows i = i0 + g, i0 + G + g, ... The G lanes of a
 // column update the shared accumulator in G ordered phases (__syncwarp
 // between them), so every bin still receives its rows in ascending order.
-// Loads for U row groups are issued before their updates.
-template <typename C, class Src, int G, int U>
+// Loads for U row groups are issued before their updates; with PIPE the
+// next U row groups' loads are also in flight during those updates.
+template <typename C, class Src, int G, int U, bool PIPE = false>
 __device__ __forceinline__ void squeeze_body(const C* __restrict__ Wx, const Src& src,
                                              const double* __restrict__ cst, int na, int N,
                                              int nbins, C* __restrict__ Tx, int* status,
@@ -86,26 +87,32 @@ __device__ __forceinline__ void squeeze_body(const C* __restrict__ Wx, const Src
   __syncwarp();
   const size_t row0 = (size_t)b * na;
   const size_t base = row0 * N + j;
-  for (int i0 = 0; i0 < na; i0 += G * U) {
+  struct Batch {
     C v[U];
     typename Src::Pre p[U];
     bool ok[U];
+  };
+  // loads of rows i0 + u*G + g, u < U
+  auto load = [&](Batch& bt, int i0) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = i0 + u * G + g;
-      ok[u] = live && i < na;
-      if (ok[u]) {
+      bt.ok[u] = live && i < na;
+      if (bt.ok[u]) {
         const size_t o = base + (size_t)i * N;
-        v[u] = Wx[o];
-        p[u] = src.pre(o, row0 + i, j);
+        bt.v[u] = Wx[o];
+        bt.p[u] = src.pre(o, row0 + i, j);
       }
     }
+  };
+  // their updates, in ascending row order per bin
+  auto update = [&](const Batch& bt, int i0) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = i0 + u * G + g;
       int k = -1;
-      if (ok[u]) {
-        k = src.bin(p[u], v[u], i);
+      if (bt.ok[u]) {
+        k = src.bin(bt.p[u], bt.v[u], i);
         if (k >= nbins) { set_status(status, DEV_BAD_BIN); k = -1; }
       }
 #pragma unroll
@@ -113,11 +120,31 @@ __device__ __forceinline__ void squeeze_body(const C* __restrict__ Wx, const Src
         if (ph == g && k >= 0) {
           C& a = acc[k * CW + c];
           const T w = cs[i];
-          a.x += v[u].x * w;
-          a.y += v[u].y * w;
+          a.x += bt.v[u].x * w;
+          a.y += bt.v[u].y * w;
         }
         if (G > 1) __syncwarp();
       }
+    }
+  };
+  constexpr int STEP = G * U;
+  if constexpr (PIPE) {
+    // two batches in flight: the next batch's loads are issued before this
+    // batch's updates
+    Batch A, B;
+    load(A, 0);
+    for (int i0 = 0; i0 < na; i0 += 2 * STEP) {
+      if (i0 + STEP < na) load(B, i0 + STEP);
+      update(A, i0);
+      if (i0 + STEP >= na) break;
+      if (i0 + 2 * STEP < na) load(A, i0 + 2 * STEP);
+      update(B, i0 + STEP);
+    }
+  } else {
+    for (int i0 = 0; i0 < na; i0 += STEP) {
+      Batch bt;
+      load(bt, i0);
+      update(bt, i0);
     }
   }
   __syncwarp();
@@ -145,7 +172,7 @@ squeeze_batch_kernel(const C* __restrict__ Wx, const uint16_t* __restrict__ idx,
   const SigDesc& d = desc[blockIdx.y];
   if ((int)blockIdx.x * (32 / G) >= d.N) return;
   IdxSrc<C> src{idx + d.idx_off, d.idx_pitch, d.N};
-  squeeze_body<C, IdxSrc<C>, G, U>(Wx + d.out_off, src, d.weights, d.na, d.N, d.nbins,
+  squeeze_body<C, IdxSrc<C>, G, U, true>(Wx + d.out_off, src, d.weights, d.na, d.N, d.nbins,
                                    Tx + d.out_off, status, 0, blockIdx.x);
 }
 
