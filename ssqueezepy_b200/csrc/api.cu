@@ -273,17 +273,18 @@ size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision) {
   if (B < 1 || Npad < 1 || na < 1) return 0;
   size_t z = min_z_bytes(B, Npad, precision);
   if (cwt_two_pass(ilog2i(Npad), precision)) {
+    const size_t budget = cwt_z_budget(ilog2i(Npad));
     const size_t per_row = (size_t)B * 2 * Npad * csize(precision);
-    size_t rows = kZBudgetBytes / per_row;
+    size_t rows = budget / per_row;
     if (rows < 2) rows = 2;  // two row tiles, one per stream
     if (rows > (size_t)na) rows = na;
     z = rows * per_row;
-    if (B > 1 && per_row > kZBudgetBytes / 2) {
+    if (B > 1 && per_row > budget / 2) {
       // signals go in chunks whose two row tiles fit the budget
       const size_t per_sig = 2 * (size_t)Npad * csize(precision);
-      size_t bc = kZBudgetBytes / 2 / per_sig;
+      size_t bc = budget / 2 / per_sig;
       if (bc < 1) bc = 1;
-      z = 2 * bc * per_sig > kZBudgetBytes ? 2 * bc * per_sig : kZBudgetBytes;
+      z = 2 * bc * per_sig > budget ? 2 * bc * per_sig : budget;
     }
     const size_t mz = min_z_bytes(B, Npad, precision);
     if (z < mz) z = mz;

@@ -32,12 +32,23 @@ inline int rows_per_tile(size_t zcap_elems, int B, int narr, int log2L, int nrow
   return (int)s;
 }
 
-// Budget of the two-pass intermediate of one ssqb_cwt call, bytes (kept
-// within the 126 MB L2 together with the spectrum and the streaming outputs).
+// Budget of the two-pass intermediate of one ssqb_cwt call, bytes. 64 MB
+// keeps it within the 126 MB L2 together with the spectrum and the streaming
+// outputs. From a padded length of 2^17 on, 256 MB (row tiles 4x larger, the
+// intermediate partly in DRAM) measured faster: cwt 1.878 -> 1.832 ms at N =
+// 160,000, 0.851 -> 0.840 at 60,000, 18.97 -> 18.74 at 2^20; at N = 10,000
+// every row then fits one tile and the two streams stop overlapping (0.139
+// -> 0.155 ms), so shorter lengths keep 64 MB.
 #ifndef SSQB_Z_MB
 #define SSQB_Z_MB 64
 #endif
+#ifndef SSQB_Z_LONG_MB
+#define SSQB_Z_LONG_MB 256
+#endif
 constexpr size_t kZBudgetBytes = (size_t)SSQB_Z_MB << 20;
+inline size_t cwt_z_budget(int log2L) {
+  return log2L >= 17 ? (size_t)SSQB_Z_LONG_MB << 20 : kZBudgetBytes;
+}
 
 // Row tiles of one transform alternate between the caller's stream and an
 // auxiliary stream of this host thread (fork and join through events), each

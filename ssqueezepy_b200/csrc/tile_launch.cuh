@@ -225,12 +225,13 @@ static int run_tile_signals(const Op& op, int B, int nrows, int log2L, C* Z, siz
   if (!SSQB_CHUNK_SIGNALS || !SSQB_DUAL_STREAM || B < 2 || !two_pass<C>(log2L) ||
       (size_t)B * per_sig <= zcap / 2)
     return run_tile<Op, C, SIGN>(op, B, nrows, log2L, Z, zcap, tb, st);
-  const size_t half = (kZBudgetBytes / sizeof(C)) / 2;
+  const size_t budget = cwt_z_budget(log2L) / sizeof(C);
+  const size_t half = budget / 2;
   size_t bc = half / per_sig;
   if (bc < 1) bc = 1;
   const int Bc = (int)bc;
   size_t cap = 2 * bc * per_sig;
-  if (cap < kZBudgetBytes / sizeof(C)) cap = kZBudgetBytes / sizeof(C);
+  if (cap < budget) cap = budget;
   if (cap > zcap) cap = zcap;
   for (int b0 = 0; b0 < B; b0 += Bc) {
     const int n = (B - b0) < Bc ? (B - b0) : Bc;
