@@ -100,9 +100,9 @@ SSQB_API int ssqb_device_status(void* stream, int* status_out);
 
 /* Workspace bytes for ssqb_cwt: the float64 padded-signal spectrum plus
  * the two-pass intermediate for two tiles of rows: a 64 MB budget (kept in
- * L2) up to Npad = 65,536, 256 MB from 131,072 on (larger row tiles measured
- * faster there). Smaller workspaces down to the minimum work too, with
- * smaller row tiles. */
+ * L2) up to Npad = 32,768, 256 MB at 65,536 and 512 MB from 131,072 on
+ * (larger row tiles measured faster there). Smaller workspaces down to the
+ * minimum work too, with smaller row tiles. */
 SSQB_API size_t ssqb_cwt_workspace_bytes(int B, int N, int Npad, int na, int precision);
 
 /* Number of kernel launches one ssqb_cwt call makes with this workspace

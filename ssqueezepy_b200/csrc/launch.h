@@ -34,20 +34,20 @@ inline int rows_per_tile(size_t zcap_elems, int B, int narr, int log2L, int nrow
 
 // Budget of the two-pass intermediate of one ssqb_cwt call, bytes. 64 MB
 // keeps it within the 126 MB L2 together with the spectrum and the streaming
-// outputs. From a padded length of 2^17 on, 256 MB (row tiles 4x larger, the
-// intermediate partly in DRAM) measured faster: cwt 1.878 -> 1.832 ms at N =
-// 160,000, 0.851 -> 0.840 at 60,000, 18.97 -> 18.74 at 2^20; at N = 10,000
-// every row then fits one tile and the two streams stop overlapping (0.139
-// -> 0.155 ms), so shorter lengths keep 64 MB.
+// outputs. Longer transforms measured faster with larger row tiles, the
+// intermediate then partly in DRAM (cwt ms, same call): at N = 160,000
+// (Npad 2^18) 64 MB 1.878, 256 MB 1.832, 512 MB 1.773; at 2^20 18.97, 18.74,
+// 18.57; at N = 40,000 (Npad 2^16) 0.472 -> 0.459 with 256 MB. At N = 10,000
+// (2^14) a large budget puts every row in one tile and the two streams stop
+// overlapping (0.139 -> 0.155 ms), so short transforms keep 64 MB.
 #ifndef SSQB_Z_MB
 #define SSQB_Z_MB 64
 #endif
-#ifndef SSQB_Z_LONG_MB
-#define SSQB_Z_LONG_MB 256
-#endif
 constexpr size_t kZBudgetBytes = (size_t)SSQB_Z_MB << 20;
 inline size_t cwt_z_budget(int log2L) {
-  return log2L >= 17 ? (size_t)SSQB_Z_LONG_MB << 20 : kZBudgetBytes;
+  if (log2L >= 17) return (size_t)512 << 20;
+  if (log2L == 16) return (size_t)256 << 20;
+  return kZBudgetBytes;
 }
 
 // Row tiles of one transform alternate between the caller's stream and an
