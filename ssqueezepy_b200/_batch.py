@@ -85,7 +85,7 @@ class SsqCwtBatch:
 
     # intermediate budgets the autotuner tries per length group, bytes, and
     # band bounds (bins; -1 = no band pass)
-    TUNE_BUDGETS = (64 << 20, 128 << 20, 256 << 20)
+    TUNE_BUDGETS = (64 << 20, 128 << 20, 256 << 20, 512 << 20)
     TUNE_BANDS = (-1, 256, 512, 1024)
 
     def __init__(self, lengths, wavelet='gmw', scales='log-piecewise', nv=32, fs=None,
