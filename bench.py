@@ -743,11 +743,13 @@ def emit(args, world, N, na, Npad, step_ms_max, value, cwt_ms, sq_ms, e2e_value,
             "stages_ms": {"cwt": cwt_avg, "squeeze": sq_avg},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": (CWT_TRAFFIC_PER_ROW_SAMPLE * na * N
-                                     if dom == 'cwt' else None),
-                         "traffic_source": "ncu dram__bytes_read+write of the fused CWT "
-                                           "call at N=40,000 (277 rows), 15.73 B per "
-                                           "(row, sample), scaled to this call",
+                         "traffic": None,
+                         "traffic_source": "not re-captured: the last ncu dram__bytes "
+                                           "read+write of the fused CWT (N=40,000, "
+                                           "%.2f B per (row, sample)) was taken with the "
+                                           "64 MB two-pass intermediate; this length now "
+                                           "uses 512 MB, part of which lives in DRAM"
+                                           % CWT_TRAFFIC_PER_ROW_SAMPLE,
                          "peak_source": src,
                          "path_frac": alg_total / (step_ms_max * 1e-3) / 1e9 / hbm},
             "compute_roofline": None if fp64_tf is None else {
